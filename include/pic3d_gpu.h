@@ -1,0 +1,165 @@
+/*
+ * pic3d_gpu.h — C ABI of the B200 implementation of the PIC3D per-timestep
+ * loop (Yee FDTD E/B half-updates, field gather + relativistic Boris push
+ * with 2nd/4th-order shapes, Esirkepov current deposition, laser /
+ * absorbing / periodic boundaries) on one GPU.
+ *
+ * Every entry point takes plain pointers and sizes and returns an int status
+ * (PIC_OK = 0).  The text of the last error is pic_last_error(ctx).  A
+ * context owns one CUDA stream on one device; calls on one context must be
+ * serialised by the caller.  Kernels never trap: a device-side problem
+ * (a particle outside the buffers, a NaN momentum, a g-factor argument
+ * outside the table, a bin overflow) sets a bit of a device status word,
+ * the offending particle is left unchanged, and the next call that
+ * synchronises (pic_synchronize, any download) returns the matching code.
+ *
+ * Layout shared with the reference (include/field.h:11-24,
+ * src/simulation.cpp:132-144): fields ex..bz are (n+2*mem)^3 buffers and
+ * jx, jy, jz, rho_electron, rho_proton are (n+2*mem+2)^3 ring buffers, each
+ * z-major with x fastest, exactly as the reference dtensor3 blocks.  Host
+ * arrays passed to upload/download are always FP64 in that layout; an FP32
+ * context converts on the device.  Particles cross the ABI as the
+ * reference's 144-byte `struct particle` (include/particle.h:9-29).
+ */
+#ifndef PIC3D_GPU_H
+#define PIC3D_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------- */
+#define PIC_OK 0
+#define PIC_EINVAL 1    /* bad argument or parameter combination */
+#define PIC_ENOMEM 2    /* device or host allocation failed */
+#define PIC_EOOB 3      /* a particle's stencil left the field buffers */
+#define PIC_ENAN 4      /* a non-finite momentum or position appeared */
+#define PIC_ETIMEOUT 5  /* a bounded device-side wait gave up */
+#define PIC_ECUDA 6     /* a CUDA runtime error */
+#define PIC_EOVERFLOW 7 /* a particle bin or buffer overflowed */
+#define PIC_ERANGE 8    /* g_factor argument outside the table (src/particle.cpp:632-636) */
+
+/* ---- array identifiers for upload / download ------------------------ */
+enum {
+    PIC_EX = 0, PIC_EY, PIC_EZ, PIC_BX, PIC_BY, PIC_BZ, /* field buffers */
+    PIC_JX, PIC_JY, PIC_JZ, PIC_RHO0, PIC_RHO1,          /* ring buffers (rho_particle[0], [1]) */
+    PIC_NARRAYS
+};
+
+/* ---- run parameters --------------------------------------------------
+ * Names follow the reference globals of src/constants.cpp:5-85
+ * (declared in include/constants.h:9-99).  One GPU holds the whole domain,
+ * so local_*cells are also the global_n* sizes.                          */
+typedef struct PicParams {
+    int32_t local_xcells, local_ycells, local_zcells;
+    int32_t mem;               /* ghost width; 2 selects 2nd-order, 4 selects 4th-order shapes (particle.cpp:184-203) */
+    int32_t rank_period[3];    /* 1: periodic pair of faces (constants.cpp:25), 0: absorbing / laser */
+    int32_t laser_polarization;/* 1 S, 2 P, 3 both (constants.cpp:60) */
+    double Pi, omega, l0, Lx;
+    double dx, dy, dz, dt, dt_half;
+    double laser_amplitude, laser_pulse_duration, laser_start_time;
+    double waist, xfocus, yfocus, zfocus, phase;
+    double E_schwinger;        /* spin precession (constants.cpp:83) */
+    double charge[2], mass[2]; /* species 0 (electrons) and 1 (protons): main.cpp:71,73 */
+    int64_t capacity[2];       /* particle capacity per species (0: sized at first upload) */
+    int32_t precision;         /* 64: FP64 everywhere; 32: FP32 fields/momenta/current, int32 cell + FP32 offsets */
+    int32_t spin;              /* 1: electron spin precession (particle.cpp:318-368); 0: skipped */
+    int32_t deposit_rho;       /* 1: per-species rho at the new positions every step (particle.cpp:503-514) */
+    int32_t laser_envelope;    /* extension: 0 sine envelope (boundary.cpp:13), 1 Gaussian with intensity FWHM laser_pulse_duration */
+    int32_t laser_profile;     /* extension: 0 Gaussian beam (boundary.cpp:38), 1 cubic-B-spline amplitude grid */
+    int32_t tile;              /* particle bin edge in cells (0: default) */
+} PicParams;
+
+typedef struct pic_ctx pic_ctx;
+
+/* Fill *p with the defaults of a 4th-order FP64 run with no laser. */
+void pic_default_params(PicParams *p);
+
+/* Create a context on `device` (initialize_domain, src/simulation.cpp:23-152:
+ * allocates and zeroes the field and ring buffers). */
+int pic_create(const PicParams *p, int device, pic_ctx **out);
+int pic_destroy(pic_ctx *ctx);
+const char *pic_last_error(const pic_ctx *ctx);
+
+/* Number of points of array `which` (field or ring buffer). */
+int pic_array_len(const pic_ctx *ctx, int which, int64_t *n);
+
+/* Host FP64 array in the reference layout <-> device. */
+int pic_upload_array(pic_ctx *ctx, int which, const double *host);
+int pic_download_array(pic_ctx *ctx, int which, double *host);
+
+/* Particles of species `kind` as reference 144-byte records (particle.h:9-29).
+ * Upload replaces the species' particles; every record must carry the
+ * species' charge and mass.  Download writes at most `cap` records and the
+ * count to *n; order is the device order (records keep their id), gamma is
+ * recomputed from the momentum as the push does (particle.cpp:309-311) and
+ * x_old..z_old are the positions before the last push (particle.cpp:267-269). */
+int pic_upload_particles(pic_ctx *ctx, int kind, const void *records, int64_t n);
+int pic_download_particles(pic_ctx *ctx, int kind, void *records, int64_t cap, int64_t *n);
+int pic_num_particles(pic_ctx *ctx, int kind, int64_t *n);
+
+/* g-factor table (the reference's g.txt, loaded by load_g_data,
+ * src/constants.cpp:114-136); needed only when spin precession meets
+ * chi >= 0.005. */
+int pic_set_g_table(pic_ctx *ctx, const double *g, int n);
+
+/* Extension: profile_n x profile_n transverse amplitude coefficients
+ * (row-major z, y) used when laser_profile = 1. */
+int pic_set_laser_profile(pic_ctx *ctx, const double *coef, int profile_n);
+
+/* ---- the reference call surface ------------------------------------- */
+/* radiating_boundary(my_rank, is_left, is_right, num_procs, step): src/boundary.cpp:42-99 */
+int pic_radiating_boundary(pic_ctx *ctx, int is_left, int is_right, int step);
+/* update_electromagnetic_fields_first(...): src/field.cpp:56-86 (with exchange_boundary_data, src/mpi_utils.cpp:9-60) */
+int pic_update_fields_first(pic_ctx *ctx);
+/* update_electromagnetic_fields_second(...): src/field.cpp:88-117 */
+int pic_update_fields_second(pic_ctx *ctx);
+/* clear_currents(): src/particle.cpp:576-592 */
+int pic_clear_currents(pic_ctx *ctx);
+/* update_particle_position_momentum(particles, n, rank, kind): src/particle.cpp:113-370,
+ * including currents_particle (src/particle.cpp:372-515) for every particle */
+int pic_update_particles(pic_ctx *ctx, int kind);
+/* exchange_particle_data(particles, n, rank, comm): src/mpi_utils.cpp:62-230 —
+ * on one GPU: removal at non-periodic global faces */
+int pic_exchange_particles(pic_ctx *ctx, int kind);
+/* exchange_currents(comm): src/particle.cpp:594-601 (exchange_boundary_current_fixed,
+ * src/mpi_utils.cpp:232-417) — periodic fold of J and rho */
+int pic_exchange_currents(pic_ctx *ctx);
+/* the t = 0 push + exchange of main.cpp:75-79 */
+int pic_initial_push(pic_ctx *ctx);
+/* `nsteps` iterations of run_main_time_loop (src/simulation.cpp:159-183);
+ * the 1-based step counter continues from the last call */
+int pic_run_steps(pic_ctx *ctx, int nsteps);
+int pic_get_step(const pic_ctx *ctx, int *step);
+int pic_set_step(pic_ctx *ctx, int step);
+
+/* Wait for the context's stream and report any device-side status. */
+int pic_synchronize(pic_ctx *ctx);
+/* The context's cudaStream_t (as void*), for callers that time or order work. */
+int pic_get_stream(const pic_ctx *ctx, void **stream);
+
+/* ---- diagnostics (FP64 device reductions, no reference counterpart) ---
+ * out[0] field energy 1/2 sum(E^2+B^2) dV over physical cells
+ * out[1] kinetic energy species 0, out[2] species 1: sum w m (gamma-1)
+ * out[3] total charge species 0, out[4] species 1 (sum of rho over physical cells times dV)
+ * out[5] max |div E - (rho0+rho1)| over physical nodes (Gauss residual) */
+#define PIC_NDIAG 6
+int pic_diagnostics(pic_ctx *ctx, double *out, int n);
+
+/* ---- per-kernel timing with CUDA events (off by default) ------------- */
+int pic_profile_enable(pic_ctx *ctx, int on);
+/* names[i] (static strings), total_ms[i] and launches[i] for up to cap kernels */
+int pic_profile_read(pic_ctx *ctx, const char **names, double *total_ms, int64_t *launches, int cap, int *count);
+int pic_profile_reset(pic_ctx *ctx);
+
+/* ---- checkpoint of the whole state (fields, currents, particles, step) */
+int pic_save(pic_ctx *ctx, const char *path);
+int pic_load(pic_ctx *ctx, const char *path);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PIC3D_GPU_H */

@@ -315,3 +315,41 @@ def load_g_table():
         # (src/constants.cpp:111-131); the file holds one more
         return np.loadtxt(REF_G_TXT)[:2849].copy()
     return None
+
+
+def _read_params_file(path):
+    p = {}
+    with open(path) as f:
+        for line in f:
+            k, v = line.split()
+            p[k] = float(v)
+    for k in ("local_xcells", "local_ycells", "local_zcells", "mem", "period_x", "period_y", "period_z",
+              "laser_polarization", "timesteps", "laser_envelope"):
+        if k in p:
+            p[k] = int(p[k])
+    return p
+
+
+def _read_particle_file(path):
+    with open(path, "rb") as f:
+        counts = np.fromfile(f, dtype="<i8", count=2)
+        return [np.fromfile(f, dtype=PARTICLE_DTYPE, count=int(c)) for c in counts]
+
+
+if __name__ == "__main__":
+    # `python oracle.py --port-time particles.bin params.txt`: time the C
+    # restatement like the reference harness's "time" mode (CPU baseline
+    # fallback when the reference build is not present).
+    import time
+    if len(sys.argv) == 4 and sys.argv[1] == "--port-time":
+        prm = _read_params_file(sys.argv[3])
+        parts = _read_particle_file(sys.argv[2])
+        o = Oracle(prm, parts)
+        o.initial()
+        n0 = int(o.s.num_particles[0] + o.s.num_particles[1])
+        t0 = time.perf_counter()
+        o.run(1, prm["timesteps"])
+        dt = time.perf_counter() - t0
+        n1 = int(o.s.num_particles[0] + o.s.num_particles[1])
+        print(json.dumps({"steps": prm["timesteps"], "particles_start": n0, "particles_end": n1,
+                          "loop_seconds": dt}))

@@ -1,0 +1,669 @@
+// C ABI of libpic3d_b200.so (include/pic3d_gpu.h): context lifetime, device
+// memory, host <-> device conversion and the per-step orchestration of the
+// reference's run_main_time_loop (src/simulation.cpp:159-183).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pic_kernels.cuh"
+
+using namespace pic;
+
+namespace {
+
+int fail(pic_ctx *c, int code, const std::string &msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                       \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess)                                                                         \
+            return fail(c, e_ == cudaErrorMemoryAllocation ? PIC_ENOMEM : PIC_ECUDA,                   \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                           \
+    } while (0)
+
+int launch_check(pic_ctx *c, const char *what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(c, PIC_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return PIC_OK;
+}
+
+size_t real_size(const pic_ctx *c) { return c->fp32 ? sizeof(float) : sizeof(double); }
+
+int bits_for(int n) {
+    int b = 1;
+    while ((1 << b) < n + 2) ++b;
+    return b;
+}
+
+template <typename T>
+int dalloc(pic_ctx *c, T **p, size_t bytes) {
+    *p = nullptr;
+    if (bytes == 0) return PIC_OK;
+    cudaError_t e = cudaMalloc((void **)p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(c, PIC_ENOMEM, std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+    }
+    return PIC_OK;
+}
+
+void free_species(Species &s) {
+    void *ptrs[] = {s.x[0], s.x[1], s.y[0], s.y[1], s.z[0], s.z[1], s.cell[0], s.cell[1], s.ox[0], s.ox[1],
+                    s.oy[0], s.oy[1], s.oz[0], s.oz[1], s.px, s.py, s.pz, s.w, s.sx, s.sy, s.sz, s.id, s.d_count};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    s = Species{};
+}
+
+int alloc_species(pic_ctx *c, int kind, int64_t cap, bool spin) {
+    Species &s = c->sp[kind];
+    free_species(s);
+    s.cap = cap;
+    const size_t rs = real_size(c), n = (size_t)(cap > 0 ? cap : 1);
+    int r = PIC_OK;
+    for (int b = 0; b < 2 && r == PIC_OK; ++b) {
+        if (c->fp32) {
+            r = r ? r : dalloc(c, &s.cell[b], n * sizeof(int));
+            r = r ? r : dalloc(c, &s.ox[b], n * sizeof(float));
+            r = r ? r : dalloc(c, &s.oy[b], n * sizeof(float));
+            r = r ? r : dalloc(c, &s.oz[b], n * sizeof(float));
+        } else {
+            r = r ? r : dalloc(c, &s.x[b], n * sizeof(double));
+            r = r ? r : dalloc(c, &s.y[b], n * sizeof(double));
+            r = r ? r : dalloc(c, &s.z[b], n * sizeof(double));
+        }
+    }
+    void **mom[4] = {&s.px, &s.py, &s.pz, &s.w};
+    for (void **m : mom) r = r ? r : dalloc(c, (char **)m, n * rs);
+    if (spin) {
+        void **sp[3] = {&s.sx, &s.sy, &s.sz};
+        for (void **m : sp) r = r ? r : dalloc(c, (char **)m, n * rs);
+    }
+    r = r ? r : dalloc(c, &s.id, n * sizeof(int));
+    r = r ? r : dalloc(c, &s.d_count, sizeof(long long));
+    if (r != PIC_OK) {
+        free_species(s);
+        return r;
+    }
+    cudaMemsetAsync(s.d_count, 0, sizeof(long long), c->stream);
+    return PIC_OK;
+}
+
+int ensure_stage(pic_ctx *c, size_t bytes) {
+    if (c->stage_bytes >= bytes) return PIC_OK;
+    if (c->d_stage) cudaFree(c->d_stage);
+    c->d_stage = nullptr;
+    c->stage_bytes = 0;
+    int r = dalloc(c, (char **)&c->d_stage, bytes);
+    if (r == PIC_OK) c->stage_bytes = bytes;
+    return r;
+}
+
+int ensure_lists(pic_ctx *c, int64_t n) {
+    if (c->list_cap >= 2 * n) return PIC_OK;
+    if (c->d_list) cudaFree(c->d_list);
+    c->d_list = nullptr;
+    c->list_cap = 0;
+    int r = dalloc(c, &c->d_list, (size_t)(2 * n) * sizeof(int));
+    if (r == PIC_OK) c->list_cap = 2 * n;
+    return r;
+}
+
+const int64_t kChunk = 1 << 20;  // particle records staged per copy
+
+int array_info(const pic_ctx *c, int which, void **dptr, long long *n) {
+    if (which < 0 || which >= PIC_NARRAYS) return PIC_EINVAL;
+    if (which < 6) {
+        *dptr = c->field[which];
+        *n = c->g.fsz;
+    } else {
+        *dptr = c->ring[which - 6];
+        *n = c->g.rsz;
+    }
+    return PIC_OK;
+}
+
+int sync_status(pic_ctx *c) {
+    CK(cudaStreamSynchronize(c->stream));
+    unsigned st = 0;
+    CK(cudaMemcpy(&st, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 2; ++k)
+        if (c->sp[k].d_count) {
+            long long n = 0;
+            CK(cudaMemcpy(&n, c->sp[k].d_count, sizeof(long long), cudaMemcpyDeviceToHost));
+            c->sp[k].n_host = n;
+        }
+    if (st) {
+        CK(cudaMemset(c->d_status, 0, sizeof(unsigned)));
+        if (st & ST_NAN) return fail(c, PIC_ENAN, "non-finite particle momentum or position (particle skipped)");
+        if (st & ST_OOB) return fail(c, PIC_EOOB, "particle stencil outside the field buffers (particle skipped)");
+        if (st & ST_CFL) return fail(c, PIC_EOOB, "particle moved a cell or more in one step (particle skipped)");
+        if (st & ST_RANGE) return fail(c, PIC_ERANGE, "g_factor argument outside the g table");
+        if (st & ST_OVERFLOW) return fail(c, PIC_EOVERFLOW, "particle bin overflow");
+        if (st & ST_TIMEOUT) return fail(c, PIC_ETIMEOUT, "device wait gave up");
+    }
+    return PIC_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+namespace pic {
+
+void prof_begin(pic_ctx *c, const char *name) {
+    if (!c->prof) return;
+    ProfEntry e{name, nullptr, nullptr};
+    cudaEventCreate(&e.a);
+    cudaEventCreate(&e.b);
+    cudaEventRecord(e.a, c->stream);
+    c->prof_events.push_back(e);
+}
+
+void prof_end(pic_ctx *c) {
+    if (!c->prof || c->prof_events.empty()) return;
+    cudaEventRecord(c->prof_events.back().b, c->stream);
+}
+
+}  // namespace pic
+
+static void prof_collect(pic_ctx *c) {
+    if (c->prof_events.empty()) return;
+    cudaStreamSynchronize(c->stream);
+    for (auto &e : c->prof_events) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e.a, e.b);
+        bool found = false;
+        for (auto &acc : c->prof_acc)
+            if (std::strcmp(acc.first, e.name) == 0) {
+                acc.second.first += ms;
+                acc.second.second += 1;
+                found = true;
+            }
+        if (!found) c->prof_acc.push_back({e.name, {ms, 1}});
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
+    c->prof_events.clear();
+}
+
+// ---------------------------------------------------------------------------
+extern "C" {
+
+void pic_default_params(PicParams *p) {
+    std::memset(p, 0, sizeof(*p));
+    p->local_xcells = p->local_ycells = p->local_zcells = 32;
+    p->mem = 4;
+    p->rank_period[0] = p->rank_period[1] = p->rank_period[2] = 1;
+    p->laser_polarization = 1;
+    p->Pi = 3.1415926536;
+    p->omega = 1.0;
+    p->l0 = 2.0 * p->Pi;
+    p->Lx = 32.0;
+    p->dx = p->dy = p->dz = 1.0;
+    p->dt = 0.95 / std::sqrt(3.0);
+    p->dt_half = p->dt / 2.0;
+    p->laser_pulse_duration = 10.0 * 2.0 * p->Pi;
+    p->waist = 3.0 * 2.0 * p->Pi;
+    p->E_schwinger = 4.1215e5;
+    p->charge[0] = -1.0;
+    p->mass[0] = 1.0;
+    p->charge[1] = 1.0;
+    p->mass[1] = 1836.0;
+    p->precision = 64;
+    p->spin = 1;
+    p->deposit_rho = 1;
+}
+
+int pic_create(const PicParams *pp, int device, pic_ctx **out) {
+    if (!pp || !out) return PIC_EINVAL;
+    *out = nullptr;
+    pic_ctx *c = new pic_ctx();
+    c->p = *pp;
+    const PicParams &p = c->p;
+    auto bad = [&](const std::string &m) {
+        std::string msg = "pic_create: " + m;
+        std::fprintf(stderr, "%s\n", msg.c_str());
+        delete c;
+        return PIC_EINVAL;
+    };
+    if (p.mem != 2 && p.mem != 4) return bad("mem must be 2 (2nd-order shape) or 4 (4th-order shape)");
+    if (p.precision != 32 && p.precision != 64) return bad("precision must be 32 or 64");
+    const int n[3] = {p.local_xcells, p.local_ycells, p.local_zcells};
+    const double d[3] = {p.dx, p.dy, p.dz};
+    for (int k = 0; k < 3; ++k) {
+        if (n[k] < 2 * p.mem + 2) return bad("every axis needs at least 2*mem+2 cells");
+        if (!(d[k] > 0.0)) return bad("cell sizes must be positive");
+        if (!(p.dt > 0.0) || !(p.dt < d[k])) return bad("dt must satisfy 0 < dt < min(dx,dy,dz) (a particle moves less than a cell per step)");
+    }
+    if (!(p.mass[0] > 0.0) || !(p.mass[1] > 0.0)) return bad("species masses must be positive");
+    c->g = make_geom(p);
+    if (c->g.rsz >= (1ll << 31)) return bad("grid too large for 32-bit buffer indexing");
+    c->fp32 = p.precision == 32;
+    c->order = p.mem == 2 ? 2 : 4;
+    c->cp.bx = bits_for(n[0]);
+    c->cp.by = bits_for(n[1]);
+    c->cp.bz = bits_for(n[2]);
+    c->cp.mx = (1u << c->cp.bx) - 1;
+    c->cp.my = (1u << c->cp.by) - 1;
+    if (c->fp32 && c->cp.bx + c->cp.by + c->cp.bz > 31) return bad("grid too large for the packed int32 cell index");
+    c->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        std::fprintf(stderr, "pic_create: cudaSetDevice(%d): %s\n", device, cudaGetErrorString(e));
+        delete c;
+        return PIC_ECUDA;
+    }
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return PIC_ECUDA;
+    }
+    const size_t rs = real_size(c);
+    int r = PIC_OK;
+    for (int k = 0; k < 6 && r == PIC_OK; ++k) r = dalloc(c, (char **)&c->field[k], (size_t)c->g.fsz * rs);
+    for (int k = 0; k < 5 && r == PIC_OK; ++k) r = dalloc(c, (char **)&c->ring[k], (size_t)c->g.rsz * rs);
+    r = r ? r : dalloc(c, &c->d_status, sizeof(unsigned));
+    r = r ? r : dalloc(c, &c->d_scratch_ll, 8 * sizeof(long long));
+    r = r ? r : dalloc(c, &c->d_diag, PIC_NDIAG * sizeof(double));
+    if (r != PIC_OK) {
+        std::fprintf(stderr, "pic_create: %s\n", c->err.c_str());
+        pic_destroy(c);
+        return r;
+    }
+    for (int k = 0; k < 6; ++k) cudaMemsetAsync(c->field[k], 0, (size_t)c->g.fsz * rs, c->stream);
+    for (int k = 0; k < 5; ++k) cudaMemsetAsync(c->ring[k], 0, (size_t)c->g.rsz * rs, c->stream);
+    cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->stream);
+    for (int k = 0; k < 2; ++k) {
+        r = alloc_species(c, k, pp->capacity[k] > 0 ? pp->capacity[k] : 0, p.spin && p.mass[k] == 1.0);
+        if (r != PIC_OK) {
+            pic_destroy(c);
+            return r;
+        }
+    }
+    e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        pic_destroy(c);
+        return PIC_ECUDA;
+    }
+    *out = c;
+    return PIC_OK;
+}
+
+int pic_destroy(pic_ctx *c) {
+    if (!c) return PIC_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto &e : c->prof_events) {
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
+    for (void *p : c->field)
+        if (p) cudaFree(p);
+    for (void *p : c->ring)
+        if (p) cudaFree(p);
+    for (auto &s : c->sp) free_species(s);
+    void *ptrs[] = {c->d_status, c->d_gtab, c->d_profile, c->d_stage, c->d_scratch_ll, c->d_list, c->d_diag};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return PIC_OK;
+}
+
+const char *pic_last_error(const pic_ctx *c) { return c ? c->err.c_str() : "no context"; }
+
+int pic_array_len(const pic_ctx *c, int which, int64_t *n) {
+    if (!c || !n) return PIC_EINVAL;
+    void *d;
+    long long len;
+    if (array_info(c, which, &d, &len) != PIC_OK) return PIC_EINVAL;
+    *n = len;
+    return PIC_OK;
+}
+
+int pic_upload_array(pic_ctx *c, int which, const double *host) {
+    if (!c || !host) return PIC_EINVAL;
+    cudaSetDevice(c->device);
+    void *d;
+    long long n;
+    if (array_info(c, which, &d, &n) != PIC_OK) return fail(c, PIC_EINVAL, "bad array id");
+    if (!c->fp32) {
+        CK(cudaMemcpyAsync(d, host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    } else {
+        int r = ensure_stage(c, (size_t)n * sizeof(double));
+        if (r) return r;
+        CK(cudaMemcpyAsync(c->d_stage, host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        launch_convert_array(c, d, c->d_stage, n, 1);
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return launch_check(c, "pic_upload_array");
+}
+
+int pic_download_array(pic_ctx *c, int which, double *host) {
+    if (!c || !host) return PIC_EINVAL;
+    cudaSetDevice(c->device);
+    void *d;
+    long long n;
+    if (array_info(c, which, &d, &n) != PIC_OK) return fail(c, PIC_EINVAL, "bad array id");
+    int st = sync_status(c);
+    if (!c->fp32) {
+        CK(cudaMemcpyAsync(host, d, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    } else {
+        int r = ensure_stage(c, (size_t)n * sizeof(double));
+        if (r) return r;
+        launch_convert_array(c, c->d_stage, d, n, 0);
+        CK(cudaMemcpyAsync(host, c->d_stage, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return st;
+}
+
+int pic_upload_particles(pic_ctx *c, int kind, const void *records, int64_t n) {
+    if (!c || kind < 0 || kind > 1 || n < 0 || (n > 0 && !records)) return PIC_EINVAL;
+    cudaSetDevice(c->device);
+    const char *rec = (const char *)records;
+    // every record of a species must carry the species' charge and mass
+    bool spin_nonzero = false;
+    for (int64_t i = 0; i < n; ++i) {
+        double q, m, s[3];
+        std::memcpy(&q, rec + 144 * i + 112, 8);
+        std::memcpy(&m, rec + 144 * i + 120, 8);
+        if (q != c->p.charge[kind] || m != c->p.mass[kind])
+            return fail(c, PIC_EINVAL, "particle record charge/mass differs from the species parameters");
+        std::memcpy(s, rec + 144 * i + 80, 24);
+        spin_nonzero = spin_nonzero || s[0] != 0.0 || s[1] != 0.0 || s[2] != 0.0;
+    }
+    Species &s = c->sp[kind];
+    bool want_spin = c->p.spin && c->p.mass[kind] == 1.0;
+    if (n > s.cap || (want_spin && !s.sx)) {
+        int r = alloc_species(c, kind, n > c->p.capacity[kind] ? n : c->p.capacity[kind], want_spin);
+        if (r) return r;
+    }
+    s.cur = 0;
+    s.spin_nonzero = spin_nonzero;
+    int r = ensure_stage(c, (size_t)(n < kChunk ? n : kChunk) * 144);
+    if (r) return r;
+    for (int64_t off = 0; off < n; off += kChunk) {
+        int64_t m = n - off < kChunk ? n - off : kChunk;
+        CK(cudaMemcpyAsync(c->d_stage, rec + 144 * off, (size_t)m * 144, cudaMemcpyHostToDevice, c->stream));
+        launch_upload_particles(c, kind, c->d_stage, m, off);
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    long long cnt = n;
+    CK(cudaMemcpyAsync(s.d_count, &cnt, sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    s.n_host = n;
+    r = ensure_lists(c, n > c->sp[1 - kind].cap ? n : c->sp[1 - kind].cap);
+    if (r) return r;
+    return launch_check(c, "pic_upload_particles");
+}
+
+int pic_download_particles(pic_ctx *c, int kind, void *records, int64_t cap, int64_t *n) {
+    if (!c || kind < 0 || kind > 1 || !n) return PIC_EINVAL;
+    cudaSetDevice(c->device);
+    int st = sync_status(c);
+    if (st == PIC_ECUDA) return st;
+    Species &s = c->sp[kind];
+    int64_t cnt = s.n_host;
+    *n = cnt;
+    if (cnt > cap) return fail(c, PIC_EINVAL, "download buffer too small");
+    if (cnt == 0) return st;
+    int r = ensure_stage(c, (size_t)(cnt < kChunk ? cnt : kChunk) * 144);
+    if (r) return r;
+    char *rec = (char *)records;
+    for (int64_t off = 0; off < cnt; off += kChunk) {
+        int64_t m = cnt - off < kChunk ? cnt - off : kChunk;
+        launch_download_particles(c, kind, c->d_stage, m, off);
+        CK(cudaMemcpyAsync(rec + 144 * off, c->d_stage, (size_t)m * 144, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    r = launch_check(c, "pic_download_particles");
+    return r ? r : st;
+}
+
+int pic_num_particles(pic_ctx *c, int kind, int64_t *n) {
+    if (!c || kind < 0 || kind > 1 || !n) return PIC_EINVAL;
+    int st = sync_status(c);
+    *n = c->sp[kind].n_host;
+    return st;
+}
+
+int pic_set_g_table(pic_ctx *c, const double *g, int n) {
+    if (!c || !g || n <= 0) return PIC_EINVAL;
+    cudaSetDevice(c->device);
+    if (c->d_gtab) cudaFree(c->d_gtab);
+    c->d_gtab = nullptr;
+    int r = dalloc(c, &c->d_gtab, (size_t)n * sizeof(double));
+    if (r) return r;
+    CK(cudaMemcpy(c->d_gtab, g, (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+    c->gtab_n = n;
+    return PIC_OK;
+}
+
+int pic_set_laser_profile(pic_ctx *c, const double *coef, int pn) {
+    if (!c || !coef || pn < 2) return PIC_EINVAL;
+    cudaSetDevice(c->device);
+    if (c->d_profile && c->profile_n != pn) {
+        cudaFree(c->d_profile);
+        c->d_profile = nullptr;
+    }
+    if (!c->d_profile) {
+        int r = dalloc(c, &c->d_profile, (size_t)pn * pn * sizeof(double));
+        if (r) return r;
+    }
+    CK(cudaMemcpyAsync(c->d_profile, coef, (size_t)pn * pn * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->profile_n = pn;
+    return PIC_OK;
+}
+
+// ---- reference call surface ---------------------------------------------
+
+int pic_radiating_boundary(pic_ctx *c, int is_left, int is_right, int step) {
+    if (!c) return PIC_EINVAL;
+    launch_radiating_boundary(c, is_left, is_right, step);
+    return launch_check(c, "radiating_boundary");
+}
+
+int pic_update_fields_first(pic_ctx *c) {
+    if (!c) return PIC_EINVAL;
+    launch_update_e(c);
+    launch_update_b(c);
+    return launch_check(c, "update_fields_first");
+}
+
+int pic_update_fields_second(pic_ctx *c) {
+    if (!c) return PIC_EINVAL;
+    launch_update_b(c);
+    launch_update_e(c);
+    return launch_check(c, "update_fields_second");
+}
+
+int pic_clear_currents(pic_ctx *c) {
+    if (!c) return PIC_EINVAL;
+    prof_begin(c, "clear_currents");
+    for (int k = 0; k < 5; ++k) CK(cudaMemsetAsync(c->ring[k], 0, (size_t)c->g.rsz * real_size(c), c->stream));
+    prof_end(c);
+    return PIC_OK;
+}
+
+int pic_update_particles(pic_ctx *c, int kind) {
+    if (!c || kind < 0 || kind > 1) return PIC_EINVAL;
+    if (c->sp[kind].n_host > 0) launch_push(c, kind);
+    return launch_check(c, "update_particles");
+}
+
+int pic_exchange_particles(pic_ctx *c, int kind) {
+    if (!c || kind < 0 || kind > 1) return PIC_EINVAL;
+    if (c->sp[kind].n_host > 0) launch_remove(c, kind);
+    return launch_check(c, "exchange_particles");
+}
+
+int pic_exchange_currents(pic_ctx *c) {
+    if (!c) return PIC_EINVAL;
+    launch_fold_currents(c);
+    return launch_check(c, "exchange_currents");
+}
+
+int pic_initial_push(pic_ctx *c) {
+    if (!c) return PIC_EINVAL;
+    int r;
+    if ((r = pic_update_particles(c, 0))) return r;
+    if ((r = pic_update_particles(c, 1))) return r;
+    if ((r = pic_exchange_particles(c, 0))) return r;
+    return pic_exchange_particles(c, 1);
+}
+
+int pic_run_steps(pic_ctx *c, int nsteps) {
+    if (!c || nsteps < 0) return PIC_EINVAL;
+    cudaSetDevice(c->device);
+    for (int t = 0; t < nsteps; ++t) {
+        c->step += 1;
+        int r;
+        if ((r = pic_radiating_boundary(c, 1, 0, c->step))) return r;
+        if ((r = pic_update_fields_first(c))) return r;
+        if ((r = pic_clear_currents(c))) return r;
+        if ((r = pic_update_particles(c, 0))) return r;
+        if ((r = pic_update_particles(c, 1))) return r;
+        if ((r = pic_exchange_particles(c, 0))) return r;
+        if ((r = pic_exchange_particles(c, 1))) return r;
+        if ((r = pic_exchange_currents(c))) return r;
+        if ((r = pic_update_fields_second(c))) return r;
+    }
+    return PIC_OK;
+}
+
+int pic_get_step(const pic_ctx *c, int *step) {
+    if (!c || !step) return PIC_EINVAL;
+    *step = c->step;
+    return PIC_OK;
+}
+
+int pic_set_step(pic_ctx *c, int step) {
+    if (!c) return PIC_EINVAL;
+    c->step = step;
+    return PIC_OK;
+}
+
+int pic_synchronize(pic_ctx *c) {
+    if (!c) return PIC_EINVAL;
+    cudaSetDevice(c->device);
+    return sync_status(c);
+}
+
+int pic_get_stream(const pic_ctx *c, void **stream) {
+    if (!c || !stream) return PIC_EINVAL;
+    *stream = (void *)c->stream;
+    return PIC_OK;
+}
+
+int pic_diagnostics(pic_ctx *c, double *out, int n) {
+    if (!c || !out || n < 1) return PIC_EINVAL;
+    cudaSetDevice(c->device);
+    launch_diagnostics(c, c->d_diag);
+    double tmp[PIC_NDIAG];
+    CK(cudaMemcpyAsync(tmp, c->d_diag, sizeof tmp, cudaMemcpyDeviceToHost, c->stream));
+    int st = sync_status(c);
+    for (int i = 0; i < n && i < PIC_NDIAG; ++i) out[i] = tmp[i];
+    return st;
+}
+
+int pic_profile_enable(pic_ctx *c, int on) {
+    if (!c) return PIC_EINVAL;
+    c->prof = on != 0;
+    return PIC_OK;
+}
+
+int pic_profile_reset(pic_ctx *c) {
+    if (!c) return PIC_EINVAL;
+    prof_collect(c);
+    c->prof_acc.clear();
+    return PIC_OK;
+}
+
+int pic_profile_read(pic_ctx *c, const char **names, double *total_ms, int64_t *launches, int cap, int *count) {
+    if (!c || !count) return PIC_EINVAL;
+    prof_collect(c);
+    int k = 0;
+    for (auto &a : c->prof_acc) {
+        if (k < cap) {
+            if (names) names[k] = a.first;
+            if (total_ms) total_ms[k] = a.second.first;
+            if (launches) launches[k] = a.second.second;
+        }
+        ++k;
+    }
+    *count = k;
+    return PIC_OK;
+}
+
+// ---- checkpoint ---------------------------------------------------------
+
+int pic_save(pic_ctx *c, const char *path) {
+    if (!c || !path) return PIC_EINVAL;
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(c, PIC_EINVAL, std::string("cannot open ") + path);
+    const char magic[8] = {'P', 'I', 'C', '3', 'D', 'B', '2', '1'};
+    std::fwrite(magic, 1, 8, f);
+    std::fwrite(&c->p, sizeof(PicParams), 1, f);
+    std::fwrite(&c->step, sizeof(int), 1, f);
+    int r = PIC_OK;
+    for (int a = 0; a < PIC_NARRAYS && r == PIC_OK; ++a) {
+        int64_t n = 0;
+        pic_array_len(c, a, &n);
+        std::vector<double> buf((size_t)n);
+        r = pic_download_array(c, a, buf.data());
+        std::fwrite(buf.data(), sizeof(double), (size_t)n, f);
+    }
+    for (int k = 0; k < 2 && r == PIC_OK; ++k) {
+        int64_t n = 0;
+        r = pic_num_particles(c, k, &n);
+        std::vector<char> rec((size_t)n * 144);
+        if (r == PIC_OK) r = pic_download_particles(c, k, rec.data(), n, &n);
+        std::fwrite(&n, sizeof(int64_t), 1, f);
+        std::fwrite(rec.data(), 1, rec.size(), f);
+    }
+    std::fclose(f);
+    return r;
+}
+
+int pic_load(pic_ctx *c, const char *path) {
+    if (!c || !path) return PIC_EINVAL;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(c, PIC_EINVAL, std::string("cannot open ") + path);
+    char magic[8];
+    PicParams p;
+    int step = 0;
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "PIC3DB21", 8) == 0 &&
+              std::fread(&p, sizeof p, 1, f) == 1 && std::fread(&step, sizeof(int), 1, f) == 1;
+    if (!ok || p.local_xcells != c->p.local_xcells || p.local_ycells != c->p.local_ycells ||
+        p.local_zcells != c->p.local_zcells || p.mem != c->p.mem) {
+        std::fclose(f);
+        return fail(c, PIC_EINVAL, "checkpoint does not match this context's grid");
+    }
+    int r = PIC_OK;
+    for (int a = 0; a < PIC_NARRAYS && r == PIC_OK; ++a) {
+        int64_t n = 0;
+        pic_array_len(c, a, &n);
+        std::vector<double> buf((size_t)n);
+        if (std::fread(buf.data(), sizeof(double), (size_t)n, f) != (size_t)n) r = fail(c, PIC_EINVAL, "short file");
+        if (r == PIC_OK) r = pic_upload_array(c, a, buf.data());
+    }
+    for (int k = 0; k < 2 && r == PIC_OK; ++k) {
+        int64_t n = 0;
+        if (std::fread(&n, sizeof n, 1, f) != 1) { r = fail(c, PIC_EINVAL, "short file"); break; }
+        std::vector<char> rec((size_t)n * 144);
+        if (std::fread(rec.data(), 1, rec.size(), f) != rec.size()) { r = fail(c, PIC_EINVAL, "short file"); break; }
+        r = pic_upload_particles(c, k, rec.data(), n);
+    }
+    std::fclose(f);
+    if (r == PIC_OK) c->step = step;
+    return r;
+}
+
+}  // extern "C"

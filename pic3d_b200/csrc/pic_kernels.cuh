@@ -1,0 +1,28 @@
+// Launchers shared between the translation units of libpic3d_b200.so.
+#pragma once
+
+#include "pic_internal.cuh"
+
+namespace pic {
+
+// profiling: CUDA events around each launch when pic_profile_enable(1)
+void prof_begin(pic_ctx *c, const char *name);
+void prof_end(pic_ctx *c);
+
+// field_kernels.cu
+void launch_update_e(pic_ctx *c);
+void launch_update_b(pic_ctx *c);
+void launch_fold_currents(pic_ctx *c);
+void launch_radiating_boundary(pic_ctx *c, int is_left, int is_right, int step);
+
+// particle_kernels.cu
+void launch_push(pic_ctx *c, int kind);
+void launch_remove(pic_ctx *c, int kind);
+void launch_upload_particles(pic_ctx *c, int kind, const void *d_records, int64_t n, int64_t offset);
+void launch_download_particles(pic_ctx *c, int kind, void *d_records, int64_t n, int64_t offset);
+void launch_convert_array(pic_ctx *c, void *dst, const void *src, long long n, int to_device);
+
+// diag_kernels.cu
+void launch_diagnostics(pic_ctx *c, double *d_out);
+
+}  // namespace pic
