@@ -106,9 +106,12 @@ class Clocks:
                 "samples": len(rows)}
 
 
+TILE = dict(tile=0, sort_interval=0)
+
+
 def make_sim(w, precision, particles, device):
     from pic3d_b200.simulation import Simulation
-    sim = Simulation(w, precision=precision, device=device)
+    sim = Simulation(w, precision=precision, device=device, **TILE)
     for k in range(2):
         sim.upload_particles(k, particles[k])
     return sim
@@ -242,7 +245,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--tile", type=int, default=0, help="shared-memory tile edge (0 default, -1 global kernel)")
+    ap.add_argument("--sort-interval", type=int, default=0)
     args = ap.parse_args()
+    TILE.update(tile=args.tile, sort_interval=args.sort_interval)
     args.warmup = max(args.warmup, 3)
 
     rank = int(os.environ.get("RANK", "0"))
@@ -303,9 +309,11 @@ def main():
     prec = args.precision
     per_particle = BYTES_PER_PARTICLE[prec] + GRID_BYTES_PER_CELL[prec] * ncell / max(npart, 1)
     roof = None
-    if top[0] == "push_gather_deposit" and top[1][1] > 0:
+    if top[0] in ("push_gather_deposit", "tile_push_gather_deposit") and top[1][1] > 0:
         avg_ms = top[1][0] / top[1][1]
-        bytes_per_launch = per_particle * npart / 2.0      # one launch per species, equal counts
+        # the global kernel runs once per species, the tiled one once for both
+        per_launch = npart / 2.0 if top[0] == "push_gather_deposit" else float(npart)
+        bytes_per_launch = per_particle * per_launch
         achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
         roof = {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
@@ -324,15 +332,17 @@ def main():
         ms32, kern32 = timed_steps(sim32, args.steps, prof=True)
         st32 = {n: sim32.download_array(n) for n in ("ex", "ey", "ez", "bx", "by", "bz")}
         err = field_rel_err(st32, st64)
-        t32 = kern32.get("push_gather_deposit", (0.0, 1))
+        kname = "tile_push_gather_deposit" if "tile_push_gather_deposit" in kern32 else "push_gather_deposit"
+        t32 = kern32.get(kname, (0.0, 1))
         avg32 = t32[0] / max(t32[1], 1)
         pp32 = BYTES_PER_PARTICLE["fp32"] + GRID_BYTES_PER_CELL["fp32"] * ncell / max(npart, 1)
-        ach32 = pp32 * npart / 2.0 / (avg32 / 1e3) / 1e9 if avg32 > 0 else None
+        per_launch32 = npart / 2.0 if kname == "push_gather_deposit" else float(npart)
+        ach32 = pp32 * per_launch32 / (avg32 / 1e3) / 1e9 if avg32 > 0 else None
         extra["fp32"] = {"value": npart_all * args.steps / (ms32 / 1e3), "ms_per_step": ms32 / args.steps,
                          "field_rel_l2_vs_fp64": err,
                          "error_note": f"E,B after {args.warmup + 1 + args.steps} steps vs the FP64 GPU run "
                                        "(itself within 1e-10/step of the FP64 oracle)",
-                         "roofline": {"kernel": "push_gather_deposit", "achieved": ach32, "peak": peak,
+                         "roofline": {"kernel": kname, "achieved": ach32, "peak": peak,
                                       "unit": "GB/s", "frac": (ach32 / peak) if ach32 else None}}
         sim32.close()
     else:
@@ -345,7 +355,7 @@ def main():
         torch.cuda.synchronize()
         host_fields = {n: np.zeros((w.nz + 2 * w.mem, w.ny + 2 * w.mem, w.nx + 2 * w.mem)) for n in
                        ("ex", "ey", "ez", "bx", "by", "bz")}
-        simE = Simulation(w, precision=prec, device=local)
+        simE = Simulation(w, precision=prec, device=local, **TILE)
         t0 = time.perf_counter()
         for n, a in host_fields.items():
             simE.upload_array(n, a)
@@ -381,6 +391,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if prec == "fp64" else "f32", "data": "synthetic",
                 "config": {"workload": w.name, "cells": [w.nx, w.ny, w.nz], "order": w.order,
+                           "tile": args.tile, "sort_interval": args.sort_interval,
                            "particles": npart, "particles_per_cell": sum(w.ppc), "boundaries": "absorbing+laser",
                            "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (particle state "
                                                                    f"{npart * BYTES_PER_PARTICLE[prec] / 1e9:.1f} GB)"},

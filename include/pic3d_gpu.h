@@ -69,7 +69,8 @@ typedef struct PicParams {
     int32_t deposit_rho;       /* 1: per-species rho at the new positions every step (particle.cpp:503-514) */
     int32_t laser_envelope;    /* extension: 0 sine envelope (boundary.cpp:13), 1 Gaussian with intensity FWHM laser_pulse_duration */
     int32_t laser_profile;     /* extension: 0 Gaussian beam (boundary.cpp:38), 1 cubic-B-spline amplitude grid */
-    int32_t tile;              /* particle bin edge in cells (0: default) */
+    int32_t tile;              /* edge of the shared-memory particle tile in cells (0: default 4, <0: no tiling) */
+    int32_t sort_interval;     /* pushes between counting sorts of the particles by cell (0: default 4) */
 } PicParams;
 
 typedef struct pic_ctx pic_ctx;

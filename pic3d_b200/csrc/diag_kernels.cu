@@ -82,9 +82,9 @@ static void diag_t(pic_ctx *c, double *d_out) {
                                                             dV, 1.0 / p.dx, 1.0 / p.dy, 1.0 / p.dz, d_out);
     for (int k = 0; k < 2; ++k) {
         Species &s = c->sp[k];
-        if (!s.px || s.n_host == 0) continue;
-        kinetic_kernel<real><<<148 * 4, 256, 0, c->stream>>>((real *)s.px, (real *)s.py, (real *)s.pz,
-                                                             (real *)s.w, s.d_count, p.mass[k], d_out + 1 + k);
+        if (!s.a.px || s.n_host == 0) continue;
+        kinetic_kernel<real><<<148 * 4, 256, 0, c->stream>>>((real *)s.a.px, (real *)s.a.py, (real *)s.a.pz,
+                                                             (real *)s.a.w, s.d_count, p.mass[k], d_out + 1 + k);
     }
 }
 

@@ -52,39 +52,59 @@ int dalloc(pic_ctx *c, T **p, size_t bytes) {
     return PIC_OK;
 }
 
-void free_species(Species &s) {
-    void *ptrs[] = {s.x[0], s.x[1], s.y[0], s.y[1], s.z[0], s.z[1], s.cell[0], s.cell[1], s.ox[0], s.ox[1],
-                    s.oy[0], s.oy[1], s.oz[0], s.oz[1], s.px, s.py, s.pz, s.w, s.sx, s.sy, s.sz, s.id, s.d_count};
+void free_arrays(PartArrays &a) {
+    void *ptrs[] = {a.x[0], a.x[1], a.y[0], a.y[1], a.z[0], a.z[1], a.cell[0], a.cell[1], a.ox[0], a.ox[1],
+                    a.oy[0], a.oy[1], a.oz[0], a.oz[1], a.px, a.py, a.pz, a.w, a.sx, a.sy, a.sz, a.id};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    a = PartArrays{};
+}
+
+void free_species(Species &s) {
+    free_arrays(s.a);
+    free_arrays(s.b);
+    if (s.d_count) cudaFree(s.d_count);
+    if (s.keys) cudaFree(s.keys);
+    if (s.offs) cudaFree(s.offs);
     s = Species{};
+}
+
+int alloc_arrays(pic_ctx *c, PartArrays &a, size_t n, bool spin) {
+    const size_t rs = real_size(c);
+    int r = PIC_OK;
+    for (int b = 0; b < 2 && r == PIC_OK; ++b) {
+        if (c->fp32) {
+            r = r ? r : dalloc(c, &a.cell[b], n * sizeof(int));
+            r = r ? r : dalloc(c, &a.ox[b], n * sizeof(float));
+            r = r ? r : dalloc(c, &a.oy[b], n * sizeof(float));
+            r = r ? r : dalloc(c, &a.oz[b], n * sizeof(float));
+        } else {
+            r = r ? r : dalloc(c, &a.x[b], n * sizeof(double));
+            r = r ? r : dalloc(c, &a.y[b], n * sizeof(double));
+            r = r ? r : dalloc(c, &a.z[b], n * sizeof(double));
+        }
+    }
+    void **mom[4] = {&a.px, &a.py, &a.pz, &a.w};
+    for (void **m : mom) r = r ? r : dalloc(c, (char **)m, n * rs);
+    if (spin) {
+        void **sp[3] = {&a.sx, &a.sy, &a.sz};
+        for (void **m : sp) r = r ? r : dalloc(c, (char **)m, n * rs);
+    }
+    r = r ? r : dalloc(c, &a.id, n * sizeof(int));
+    return r;
 }
 
 int alloc_species(pic_ctx *c, int kind, int64_t cap, bool spin) {
     Species &s = c->sp[kind];
     free_species(s);
     s.cap = cap;
-    const size_t rs = real_size(c), n = (size_t)(cap > 0 ? cap : 1);
-    int r = PIC_OK;
-    for (int b = 0; b < 2 && r == PIC_OK; ++b) {
-        if (c->fp32) {
-            r = r ? r : dalloc(c, &s.cell[b], n * sizeof(int));
-            r = r ? r : dalloc(c, &s.ox[b], n * sizeof(float));
-            r = r ? r : dalloc(c, &s.oy[b], n * sizeof(float));
-            r = r ? r : dalloc(c, &s.oz[b], n * sizeof(float));
-        } else {
-            r = r ? r : dalloc(c, &s.x[b], n * sizeof(double));
-            r = r ? r : dalloc(c, &s.y[b], n * sizeof(double));
-            r = r ? r : dalloc(c, &s.z[b], n * sizeof(double));
-        }
+    const size_t n = (size_t)(cap > 0 ? cap : 1);
+    int r = alloc_arrays(c, s.a, n, spin);
+    if (c->tile > 0 && cap > 0) {
+        r = r ? r : alloc_arrays(c, s.b, n, spin);
+        r = r ? r : dalloc(c, &s.keys, n * sizeof(int));
+        r = r ? r : dalloc(c, &s.offs, (size_t)(c->nkeys + 1) * sizeof(unsigned));
     }
-    void **mom[4] = {&s.px, &s.py, &s.pz, &s.w};
-    for (void **m : mom) r = r ? r : dalloc(c, (char **)m, n * rs);
-    if (spin) {
-        void **sp[3] = {&s.sx, &s.sy, &s.sz};
-        for (void **m : sp) r = r ? r : dalloc(c, (char **)m, n * rs);
-    }
-    r = r ? r : dalloc(c, &s.id, n * sizeof(int));
     r = r ? r : dalloc(c, &s.d_count, sizeof(long long));
     if (r != PIC_OK) {
         free_species(s);
@@ -236,7 +256,11 @@ int pic_create(const PicParams *pp, int device, pic_ctx **out) {
     const int n[3] = {p.local_xcells, p.local_ycells, p.local_zcells};
     const double d[3] = {p.dx, p.dy, p.dz};
     for (int k = 0; k < 3; ++k) {
-        if (n[k] < 2 * p.mem + 2) return bad("every axis needs at least 2*mem+2 cells");
+        // periodic axes: the ghost slabs of both sides must not overlap
+        // (the reference halo exchange needs the same); absorbing axes: the
+        // x-max boundary column local_xcells+1 must not meet the x-min one
+        if (p.rank_period[k] && n[k] < 2 * p.mem + 2) return bad("a periodic axis needs at least 2*mem+2 cells");
+        if (!p.rank_period[k] && n[k] < p.mem) return bad("an absorbing axis needs at least mem cells");
         if (!(d[k] > 0.0)) return bad("cell sizes must be positive");
         if (!(p.dt > 0.0) || !(p.dt < d[k])) return bad("dt must satisfy 0 < dt < min(dx,dy,dz) (a particle moves less than a cell per step)");
     }
@@ -251,6 +275,15 @@ int pic_create(const PicParams *pp, int device, pic_ctx **out) {
     c->cp.mx = (1u << c->cp.bx) - 1;
     c->cp.my = (1u << c->cp.by) - 1;
     if (c->fp32 && c->cp.bx + c->cp.by + c->cp.bz > 31) return bad("grid too large for the packed int32 cell index");
+    // tiling: 0 -> default edge of 4 cells, < 0 -> global-memory kernel only
+    c->tile = p.tile == 0 ? 4 : (p.tile < 0 ? 0 : p.tile);
+    c->sort_interval = p.sort_interval > 0 ? p.sort_interval : 4;
+    if (c->tile > 0) {
+        for (int d = 0; d < 3; ++d) c->ntile[d] = (n[d] + c->tile - 1) / c->tile;
+        c->nkeys = (long long)c->ntile[0] * c->ntile[1] * c->ntile[2] * c->tile * c->tile * c->tile;
+        if (c->nkeys >= (1ll << 31)) return bad("too many sort keys");
+        if (tile_smem_bytes(c) > 227 * 1024) return bad("tile too large for shared memory");
+    }
     c->device = device;
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) {
@@ -270,6 +303,10 @@ int pic_create(const PicParams *pp, int device, pic_ctx **out) {
     r = r ? r : dalloc(c, &c->d_status, sizeof(unsigned));
     r = r ? r : dalloc(c, &c->d_scratch_ll, 8 * sizeof(long long));
     r = r ? r : dalloc(c, &c->d_diag, PIC_NDIAG * sizeof(double));
+    if (c->tile > 0) {
+        r = r ? r : dalloc(c, &c->d_hist, (size_t)(c->nkeys + 1) * sizeof(unsigned));
+        r = r ? r : dalloc(c, &c->d_blocksums, (size_t)(c->nkeys / 4096 + 2) * sizeof(unsigned));
+    }
     if (r != PIC_OK) {
         std::fprintf(stderr, "pic_create: %s\n", c->err.c_str());
         pic_destroy(c);
@@ -307,7 +344,8 @@ int pic_destroy(pic_ctx *c) {
     for (void *p : c->ring)
         if (p) cudaFree(p);
     for (auto &s : c->sp) free_species(s);
-    void *ptrs[] = {c->d_status, c->d_gtab, c->d_profile, c->d_stage, c->d_scratch_ll, c->d_list, c->d_diag};
+    void *ptrs[] = {c->d_status, c->d_gtab, c->d_profile, c->d_stage, c->d_scratch_ll, c->d_list, c->d_diag,
+                    c->d_hist, c->d_blocksums};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -380,11 +418,12 @@ int pic_upload_particles(pic_ctx *c, int kind, const void *records, int64_t n) {
     }
     Species &s = c->sp[kind];
     bool want_spin = c->p.spin && c->p.mass[kind] == 1.0;
-    if (n > s.cap || (want_spin && !s.sx)) {
+    if (n > s.cap || (want_spin && !s.a.sx)) {
         int r = alloc_species(c, kind, n > c->p.capacity[kind] ? n : c->p.capacity[kind], want_spin);
         if (r) return r;
     }
     s.cur = 0;
+    s.sorted = false;
     s.spin_nonzero = spin_nonzero;
     int r = ensure_stage(c, (size_t)(n < kChunk ? n : kChunk) * 144);
     if (r) return r;
@@ -494,8 +533,23 @@ int pic_clear_currents(pic_ctx *c) {
 
 int pic_update_particles(pic_ctx *c, int kind) {
     if (!c || kind < 0 || kind > 1) return PIC_EINVAL;
-    if (c->sp[kind].n_host > 0) launch_push(c, kind);
+    if (c->sp[kind].n_host > 0) {
+        if (c->tile > 0) launch_tile_push(c, 1 << kind);
+        else launch_push(c, kind);
+    }
     return launch_check(c, "update_particles");
+}
+
+// both species in one launch when tiled (the two pushes only read the
+// fields and add into J, so fusing them changes nothing but the order of
+// the additions)
+static int push_both(pic_ctx *c) {
+    if (c->tile > 0) {
+        if (c->sp[0].n_host > 0 || c->sp[1].n_host > 0) launch_tile_push(c, 3);
+        return launch_check(c, "update_particles");
+    }
+    int r = pic_update_particles(c, 0);
+    return r ? r : pic_update_particles(c, 1);
 }
 
 int pic_exchange_particles(pic_ctx *c, int kind) {
@@ -513,8 +567,7 @@ int pic_exchange_currents(pic_ctx *c) {
 int pic_initial_push(pic_ctx *c) {
     if (!c) return PIC_EINVAL;
     int r;
-    if ((r = pic_update_particles(c, 0))) return r;
-    if ((r = pic_update_particles(c, 1))) return r;
+    if ((r = push_both(c))) return r;
     if ((r = pic_exchange_particles(c, 0))) return r;
     return pic_exchange_particles(c, 1);
 }
@@ -528,8 +581,7 @@ int pic_run_steps(pic_ctx *c, int nsteps) {
         if ((r = pic_radiating_boundary(c, 1, 0, c->step))) return r;
         if ((r = pic_update_fields_first(c))) return r;
         if ((r = pic_clear_currents(c))) return r;
-        if ((r = pic_update_particles(c, 0))) return r;
-        if ((r = pic_update_particles(c, 1))) return r;
+        if ((r = push_both(c))) return r;
         if ((r = pic_exchange_particles(c, 0))) return r;
         if ((r = pic_exchange_particles(c, 1))) return r;
         if ((r = pic_exchange_currents(c))) return r;

@@ -83,20 +83,26 @@ __device__ __forceinline__ void shape_weights(real d, real (&w)[5]) {
 //   FP64: x,y,z absolute cell coordinates as in the reference, two buffers
 //         (current and previous positions) that swap every push.
 //   FP32: packed int32 cell index + three FP32 in-cell offsets in [0,1).
+struct PartArrays {
+    double *x[2] = {nullptr, nullptr}, *y[2] = {nullptr, nullptr}, *z[2] = {nullptr, nullptr};
+    int *cell[2] = {nullptr, nullptr};
+    float *ox[2] = {nullptr, nullptr}, *oy[2] = {nullptr, nullptr}, *oz[2] = {nullptr, nullptr};
+    void *px = nullptr, *py = nullptr, *pz = nullptr, *w = nullptr;   // double* or float* by precision
+    void *sx = nullptr, *sy = nullptr, *sz = nullptr;                 // spins (only when spin is on)
+    int *id = nullptr;
+};
+
 struct Species {
     int64_t cap = 0;
     int64_t n_host = 0;      // host copy of the count (upper bound between syncs)
     long long *d_count = nullptr;
     int cur = 0;             // which position buffer is current
-    // FP64 positions
-    double *x[2] = {nullptr, nullptr}, *y[2] = {nullptr, nullptr}, *z[2] = {nullptr, nullptr};
-    // FP32 positions
-    int *cell[2] = {nullptr, nullptr};
-    float *ox[2] = {nullptr, nullptr}, *oy[2] = {nullptr, nullptr}, *oz[2] = {nullptr, nullptr};
-    // momenta and weight (double* or float* by precision)
-    void *px = nullptr, *py = nullptr, *pz = nullptr, *w = nullptr;
-    void *sx = nullptr, *sy = nullptr, *sz = nullptr;   // spins (only when spin is on)
-    int *id = nullptr;
+    PartArrays a;            // the particles
+    PartArrays b;            // destination of the counting sort (same shapes)
+    int *keys = nullptr;     // per-particle sort key
+    unsigned *offs = nullptr;  // per-key start offsets after the last sort (nkeys + 1)
+    bool sorted = false;     // offs describes the current order
+    int pushes_since_sort = 0;
     bool spin_nonzero = false;
 };
 
@@ -146,6 +152,14 @@ struct pic_ctx {
     int *d_list = nullptr;               // compaction index lists
     int64_t list_cap = 0;
     double *d_diag = nullptr;
+    // tiling / sorting
+    int tile = 0;                        // tile edge in cells (0: global-memory kernel only)
+    int ntile[3] = {0, 0, 0};
+    long long nkeys = 0;                 // ntiles * tile^3
+    unsigned *d_hist = nullptr;          // nkeys + 1
+    unsigned *d_blocksums = nullptr;
+    int sort_interval = 4;
+    int steps_since_sort = 0;
     int step = 0;
     std::string err;
     // profiling

@@ -22,6 +22,11 @@ void launch_upload_particles(pic_ctx *c, int kind, const void *d_records, int64_
 void launch_download_particles(pic_ctx *c, int kind, void *d_records, int64_t n, int64_t offset);
 void launch_convert_array(pic_ctx *c, void *dst, const void *src, long long n, int to_device);
 
+// tile_kernels.cu
+void launch_sort(pic_ctx *c, int kind);
+void launch_tile_push(pic_ctx *c, int mask);
+size_t tile_smem_bytes(const pic_ctx *c);
+
 // diag_kernels.cu
 void launch_diagnostics(pic_ctx *c, double *d_out);
 

@@ -1,0 +1,453 @@
+// Per-particle body of update_particle_position_momentum
+// (src/particle.cpp:113-370) with currents_particle (:372-515), shared by
+// the global-memory kernel and the tiled shared-memory kernel.  Field reads
+// and current adds go through `View`s, so the same code addresses either
+// the global buffers or a CTA's shared-memory tile.
+#pragma once
+
+#include <cuda/std/type_traits>
+
+#include "pic_internal.cuh"
+
+namespace pic {
+
+template <typename real>
+struct PushArgs {
+    Geom g;
+    const real *ex, *ey, *ez, *bx, *by, *bz;
+    real *jx, *jy, *jz, *rho;
+    const long long *count;
+    // FP64 positions (cur -> nxt)
+    double *x0, *y0, *z0;
+    double *x1, *y1, *z1;
+    // FP32 positions
+    int *c0;
+    const float *ox0, *oy0, *oz0;
+    int *c1;
+    float *ox1, *oy1, *oz1;
+    CellPack cp;
+    real *px, *py, *pz;
+    const real *w;
+    real *sx, *sy, *sz;
+    const double *gtab;
+    int gtab_n;
+    real qm;                 // charge / mass * dt_half (particle.cpp:271)
+    real charge;
+    real dt_d[3];            // dt / dx, dt / dy, dt / dz
+    double dt_s, dxs[3];     // dt and dx, dy, dz
+    real d_dt[3];            // dx / dt, dy / dt, dz / dt (particle.cpp:423-425)
+    double E_schwinger, dt_half_d, charge_d, mass_d;
+    int electron;            // spin precession applies to this species (particle.cpp:318-319)
+    unsigned *status;
+};
+
+// A 3D array seen through buffer coordinates: element (k, j, i) is at
+// p[k*sz + j*sy + i + o].
+template <typename T>
+struct View {
+    T *p;
+    int sy, sz, o;
+    __device__ __forceinline__ T *at(int k, int j, int i) const { return p + (k * sz + j * sy + i + o); }
+};
+
+__device__ __forceinline__ void set_status(unsigned *s, unsigned bit) { atomicOr(s, bit); }
+
+// g_factor lookup (src/particle.cpp:603-637)
+__device__ __forceinline__ double g_factor_dev(const double *tab, int n, double x, unsigned *status) {
+    int idx;
+    if (x < 0.005 && x >= 0.0) return 2.003219;
+    if (x >= 0.005 && x < 0.01) idx = (int)((x - 0.005) / 0.0001);
+    else if (x >= 0.01 && x < 1) idx = (int)((x - 0.01) / 0.01) + 50;
+    else if (x >= 1 && x < 10) idx = (int)((x - 1.0) / 0.01) + 150;
+    else if (x >= 10 && x < 20) idx = (int)((x - 10.0) / 0.01) + 1050;
+    else if (x >= 20 && x <= 100) idx = (int)((x - 20.0) / 0.1) + 2050;
+    else { set_status(status, ST_RANGE); return 2.003219; }
+    if (!tab || idx < 0 || idx >= n) { set_status(status, ST_RANGE); return 2.003219; }
+    return tab[idx];
+}
+
+// factorised P^3 gather of one staggered component, starting at (k0,j0,i0)
+template <typename real, int P, bool LDG>
+__device__ __forceinline__ real gather(const View<const real> &v, int i0, int j0, int k0, const real (&wx)[P],
+                                       const real (&wy)[P], const real (&wz)[P]) {
+    const real *base = v.at(k0, j0, i0);
+    real acc = 0;
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+        real acck = 0;
+#pragma unroll
+        for (int j = 0; j < P; ++j) {
+            const real *row = base + k * v.sz + j * v.sy;
+            real s = 0;
+#pragma unroll
+            for (int i = 0; i < P; ++i) s += wx[i] * (LDG ? __ldg(row + i) : row[i]);
+            acck += wy[j] * s;
+        }
+        acc += wz[k] * acck;
+    }
+    return acc;
+}
+
+// 1D pieces of the Esirkepov weights over the union span of the old and new
+// supports (src/particle.cpp:403-419): s0 = old shape, ds = new - old,
+// zero outside each support.  |i2 - i1| <= 1 (checked by the caller).
+template <typename real, int P>
+__device__ __forceinline__ void span1d(int i1, const real (&w0)[P], int i2, const real (&w1)[P], int &base,
+                                       int &len, real (&s0)[P + 1], real (&ds)[P + 1]) {
+    constexpr int H = P / 2;
+    const int lo = min(i1, i2);
+    base = lo - H;
+    len = P + abs(i2 - i1);
+    const bool o0 = i1 != lo, o1 = i2 != lo;
+#pragma unroll
+    for (int a = 0; a <= P; ++a) {
+        real v0 = o0 ? (a >= 1 ? w0[a - 1] : real(0)) : (a < P ? w0[a] : real(0));
+        real v1 = o1 ? (a >= 1 ? w1[a - 1] : real(0)) : (a < P ? w1[a] : real(0));
+        s0[a] = v0;
+        ds[a] = v1 - v0;
+    }
+}
+
+__device__ __forceinline__ void atomic_add(double *p, double v) { atomicAdd(p, v); }
+__device__ __forceinline__ void atomic_add(float *p, float v) { atomicAdd(p, v); }
+
+// Esirkepov deposit (src/particle.cpp:427-500) and rho (:503-514).  The
+// last point of each running sum (the sum of all ds, zero up to rounding)
+// is not added.
+template <typename real, int P>
+__device__ __forceinline__ void deposit(const View<real> &vj0, real *jx, real *jy, real *jz, real *rho,
+                                        const real (&dxdt)[3], const int (&i1)[3], const real (&w0)[3][P],
+                                        const int (&i2)[3], const real (&w1)[3][P], real qw) {
+    constexpr int H = P / 2;
+    int base[3], len[3];
+    real s0[3][P + 1], ds[3][P + 1];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) span1d<real, P>(i1[d], w0[d], i2[d], w1[d], base[d], len[d], s0[d], ds[d]);
+    const real third = real(1.0 / 3.0), half = real(0.5);
+    const real cx = qw * dxdt[0], cy = qw * dxdt[1], cz = qw * dxdt[2];
+    const int rx = vj0.sy, rxy = vj0.sz;
+    const int r0 = base[2] * rxy + base[1] * rx + base[0] + vj0.o;
+#pragma unroll
+    for (int k = 0; k <= P; ++k) {
+        if (k >= len[2]) break;
+#pragma unroll
+        for (int j = 0; j <= P; ++j) {
+            if (j >= len[1]) break;
+            real wyz = s0[1][j] * s0[2][k] + half * ds[1][j] * s0[2][k] + half * s0[1][j] * ds[2][k] +
+                       third * ds[1][j] * ds[2][k];
+            real acc = 0;
+            real *row = jx + r0 + k * rxy + j * rx;
+#pragma unroll
+            for (int i = 0; i < P; ++i) {
+                if (i >= len[0] - 1) break;
+                acc += ds[0][i];
+                atomic_add(row + i, -cx * acc * wyz);
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k <= P; ++k) {
+        if (k >= len[2]) break;
+#pragma unroll
+        for (int i = 0; i <= P; ++i) {
+            if (i >= len[0]) break;
+            real wxz = s0[0][i] * s0[2][k] + half * ds[0][i] * s0[2][k] + half * s0[0][i] * ds[2][k] +
+                       third * ds[0][i] * ds[2][k];
+            real acc = 0;
+            real *col = jy + r0 + k * rxy + i;
+#pragma unroll
+            for (int j = 0; j < P; ++j) {
+                if (j >= len[1] - 1) break;
+                acc += ds[1][j];
+                atomic_add(col + j * rx, -cy * acc * wxz);
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j <= P; ++j) {
+        if (j >= len[1]) break;
+#pragma unroll
+        for (int i = 0; i <= P; ++i) {
+            if (i >= len[0]) break;
+            real wxy = s0[0][i] * s0[1][j] + half * ds[0][i] * s0[1][j] + half * s0[0][i] * ds[1][j] +
+                       third * ds[0][i] * ds[1][j];
+            real acc = 0;
+            real *col = jz + r0 + j * rx + i;
+#pragma unroll
+            for (int k = 0; k < P; ++k) {
+                if (k >= len[2] - 1) break;
+                acc += ds[2][k];
+                atomic_add(col + k * rxy, -cz * acc * wxy);
+            }
+        }
+    }
+    if (rho) {
+        real *rb = rho + (i2[2] - H) * rxy + (i2[1] - H) * rx + (i2[0] - H) + vj0.o;
+#pragma unroll
+        for (int k = 0; k < P; ++k)
+#pragma unroll
+            for (int j = 0; j < P; ++j) {
+                real wjk = qw * w1[1][j] * w1[2][k];
+#pragma unroll
+                for (int i = 0; i < P; ++i) atomic_add(rb + k * rxy + j * rx + i, wjk * w1[0][i]);
+            }
+    }
+}
+
+// Decoded old position of particle p: primal / dual buffer index and
+// offset per axis.  FP64 applies the push-time periodic wrap
+// (particle.cpp:123-167) and writes the wrapped position back.
+template <typename real>
+struct OldPos {
+    int ip[3], id[3];
+    real dp[3], dd[3];
+    double xd[3];
+    int cc[3];
+    real oo[3];
+};
+
+template <typename real>
+__device__ __forceinline__ void decode_old(const PushArgs<real> &a, long long p, OldPos<real> &o) {
+    constexpr bool F64 = cuda::std::is_same<real, double>::value;
+    const Geom &g = a.g;
+    if constexpr (F64) {
+        o.xd[0] = a.x0[p];
+        o.xd[1] = a.y0[p];
+        o.xd[2] = a.z0[p];
+        bool wrapped = false;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if (g.per[d]) {
+                if (o.xd[d] < 0.0) { o.xd[d] += g.n[d]; wrapped = true; }
+                if (o.xd[d] > (double)g.n[d]) { o.xd[d] -= g.n[d]; wrapped = true; }
+            }
+        }
+        if (wrapped) {
+            a.x0[p] = o.xd[0];
+            a.y0[p] = o.xd[1];
+            a.z0[p] = o.xd[2];
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double xc = o.xd[d] - (double)(1 - g.mem);
+            o.ip[d] = (int)(xc + 0.5);
+            o.dp[d] = xc - (double)o.ip[d];
+            o.id[d] = (int)xc;
+            o.dd[d] = (xc - 0.5) - (double)o.id[d];
+        }
+    } else {
+        a.cp.unpack(a.c0[p], o.cc[0], o.cc[1], o.cc[2]);
+        o.oo[0] = a.ox0[p];
+        o.oo[1] = a.oy0[p];
+        o.oo[2] = a.oz0[p];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            int b = o.cc[d] + g.mem - 1;
+            bool up = o.oo[d] >= 0.5f;
+            o.ip[d] = b + (up ? 1 : 0);
+            o.dp[d] = up ? o.oo[d] - 1.0f : o.oo[d];
+            o.id[d] = b;
+            o.dd[d] = o.oo[d] - 0.5f;
+        }
+    }
+}
+
+// Everything after the position decode: gather, Boris, move, deposit,
+// store, spin.  fv: the six field views; jv: view for the current arrays
+// (jx..rho share its strides).
+template <typename real, int P, bool SPIN, bool LDG>
+__device__ __forceinline__ void push_body(const PushArgs<real> &a, long long p, const OldPos<real> &o,
+                                          const View<const real> (&fv)[6], const View<real> &jv, real *jx,
+                                          real *jy, real *jz, real *rho) {
+    constexpr bool F64 = cuda::std::is_same<real, double>::value;
+    constexpr int H = P / 2;
+    const Geom &g = a.g;
+    real wp[3][P], wd[3][P];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        shape_weights(o.dp[d], wp[d]);
+        shape_weights(o.dd[d], wd[d]);
+    }
+    // gather with Yee staggering (particle.cpp:207-259)
+    const int *ip = o.ip, *id = o.id;
+    real e0 = gather<real, P, LDG>(fv[0], id[0] - H, ip[1] - H, ip[2] - H, wd[0], wp[1], wp[2]);
+    real e1 = gather<real, P, LDG>(fv[1], ip[0] - H, id[1] - H, ip[2] - H, wp[0], wd[1], wp[2]);
+    real e2 = gather<real, P, LDG>(fv[2], ip[0] - H, ip[1] - H, id[2] - H, wp[0], wp[1], wd[2]);
+    real b0 = gather<real, P, LDG>(fv[3], ip[0] - H, id[1] - H, id[2] - H, wp[0], wd[1], wd[2]);
+    real b1 = gather<real, P, LDG>(fv[4], id[0] - H, ip[1] - H, id[2] - H, wd[0], wp[1], wd[2]);
+    real b2 = gather<real, P, LDG>(fv[5], id[0] - H, id[1] - H, ip[2] - H, wd[0], wd[1], wp[2]);
+    // Boris (particle.cpp:271-306)
+    const real qm = a.qm;
+    real ex_p = e0 * qm, ey_p = e1 * qm, ez_p = e2 * qm;
+    real bx_p = b0 * qm, by_p = b1 * qm, bz_p = b2 * qm;
+    real px1 = a.px[p] + ex_p, py1 = a.py[p] + ey_p, pz1 = a.pz[p] + ez_p;
+    real gm1 = sqrt(real(1) + (px1 * px1 + py1 * py1 + pz1 * pz1));
+    real tx = bx_p / gm1, ty = by_p / gm1, tz = bz_p / gm1;
+    real tt = real(2) / (real(1) + tx * tx + ty * ty + tz * tz);
+    real sx = tx * tt, sy = ty * tt, sz = tz * tt;
+    real px2 = px1 + (py1 * tz - pz1 * ty);
+    real py2 = py1 + (pz1 * tx - px1 * tz);
+    real pz2 = pz1 + (px1 * ty - py1 * tx);
+    real pxn = px1 + (py2 * sz - pz2 * sy) + ex_p;
+    real pyn = py1 + (pz2 * sx - px2 * sz) + ey_p;
+    real pzn = pz1 + (px2 * sy - py2 * sx) + ez_p;
+    real gam = sqrt(real(1) + (pxn * pxn + pyn * pyn + pzn * pzn));
+    // move in cell units (particle.cpp:313-315)
+    int i2[3];
+    real d2[3];
+    double xn[3];
+    int cn[3];
+    real on[3];
+    if constexpr (F64) {
+        xn[0] = o.xd[0] + (double)pxn / (double)gam * a.dt_s / a.dxs[0];
+        xn[1] = o.xd[1] + (double)pyn / (double)gam * a.dt_s / a.dxs[1];
+        xn[2] = o.xd[2] + (double)pzn / (double)gam * a.dt_s / a.dxs[2];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double xc = xn[d] - (double)(1 - g.mem);
+            i2[d] = (int)(xc + 0.5);
+            d2[d] = xc - (double)i2[d];
+        }
+    } else {
+        const real disp[3] = {pxn / gam * a.dt_d[0], pyn / gam * a.dt_d[1], pzn / gam * a.dt_d[2]};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            real q = o.oo[d] + disp[d];
+            int s = 0;
+            if (q >= real(1)) { q -= real(1); s = 1; }
+            else if (q < real(0)) {
+                q += real(1);
+                s = -1;
+                if (q >= real(1)) { q = real(0); s = 0; }
+            }
+            cn[d] = o.cc[d] + s;
+            on[d] = q;
+            int b = cn[d] + g.mem - 1;
+            bool up = q >= real(0.5);
+            i2[d] = b + (up ? 1 : 0);
+            d2[d] = up ? q - real(1) : q;
+        }
+    }
+    bool fin = isfinite(pxn) && isfinite(pyn) && isfinite(pzn);
+    bool cfl = abs(i2[0] - ip[0]) <= 1 && abs(i2[1] - ip[1]) <= 1 && abs(i2[2] - ip[2]) <= 1;
+    if (!fin || !cfl) {
+        set_status(a.status, fin ? ST_CFL : ST_NAN);
+        return;
+    }
+    real w1[3][P];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) shape_weights(d2[d], w1[d]);
+    const real qw = a.charge * a.w[p];
+    deposit<real, P>(jv, jx, jy, jz, rho, a.d_dt, o.ip, wp, i2, w1, qw);
+    // store
+    a.px[p] = pxn;
+    a.py[p] = pyn;
+    a.pz[p] = pzn;
+    if constexpr (F64) {
+        a.x1[p] = xn[0];
+        a.y1[p] = xn[1];
+        a.z1[p] = xn[2];
+    } else {
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            if (g.per[d]) cn[d] = cn[d] < 0 ? cn[d] + g.n[d] : (cn[d] >= g.n[d] ? cn[d] - g.n[d] : cn[d]);
+        a.c1[p] = a.cp.pack(cn[0], cn[1], cn[2]);
+        a.ox1[p] = on[0];
+        a.oy1[p] = on[1];
+        a.oz1[p] = on[2];
+    }
+    // electron spin precession (particle.cpp:318-368)
+    if constexpr (SPIN) {
+        if (a.electron) {
+            double exq = e0, eyq = e1, ezq = e2, bxq = b0, byq = b1, bzq = b2;
+            double g0 = gam;
+            double vx = (double)pxn / g0, vy = (double)pyn / g0, vz = (double)pzn / g0;
+            double pe = vx * exq + vy * eyq + vz * ezq;
+            double fx = exq + vy * bzq - vz * byq;
+            double fy = eyq + vz * bxq - vx * bzq;
+            double fz = ezq + vx * byq - vy * bxq;
+            double chi = fx * fx + fy * fy + fz * fz - pe * pe;
+            chi = chi > 0.0 ? chi : 0.0;
+            chi = sqrt(chi) / a.E_schwinger * g0;
+            double gf = g_factor_dev(a.gtab, a.gtab_n, chi, a.status);
+            double al = -(gf / 2.0 - 1.0) * g0 / (1.0 + g0);
+            double be = (gf / 2.0 - 1.0) + 1.0 / g0;
+            double gg = gf / 2.0 - g0 / (1.0 + g0);
+            double vb = vx * bxq + vy * byq + vz * bzq;
+            double ox = al * vb * vx + be * bxq + gg * (vy * ezq - vz * eyq);
+            double oy = al * vb * vy + be * byq + gg * (vz * exq - vx * ezq);
+            double oz = al * vb * vz + be * bzq + gg * (vx * eyq - vy * exq);
+            double q2 = a.charge_d / a.mass_d * a.dt_half_d;
+            double ux = ox * q2, uy = oy * q2, uz = oz * q2;
+            double t2 = 2.0 / (1.0 + ux * ux + uy * uy + uz * uz);
+            double s_x = a.sx[p], s_y = a.sy[p], s_z = a.sz[p];
+            double rx = s_x + (s_y * uz - s_z * uy);
+            double ry = s_y + (s_z * ux - s_x * uz);
+            double rz = s_z + (s_x * uy - s_y * ux);
+            a.sx[p] = (real)(s_x + (ry * uz - rz * uy) * t2);
+            a.sy[p] = (real)(s_y + (rz * ux - rx * uz) * t2);
+            a.sz[p] = (real)(s_z + (rx * uy - ry * ux) * t2);
+        }
+    }
+}
+
+// bounds check of the old position against the global buffers: the whole
+// gather and deposit stencil must stay inside (see the ring / field extents)
+template <typename real>
+__device__ __forceinline__ bool in_buffers(const Geom &g, const OldPos<real> &o, int H) {
+    bool ok = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) ok = ok && o.id[d] >= H && o.ip[d] <= g.f[d] - 1 - H;
+    return ok;
+}
+
+template <typename real>
+__device__ __forceinline__ void global_views(const PushArgs<real> &a, View<const real> (&fv)[6], View<real> &jv) {
+    const Geom &g = a.g;
+    const real *f[6] = {a.ex, a.ey, a.ez, a.bx, a.by, a.bz};
+#pragma unroll
+    for (int c = 0; c < 6; ++c) fv[c] = View<const real>{f[c], g.f[0], g.fxy, 0};
+    jv = View<real>{a.jx, g.r[0], g.rxy, g.rxy + g.r[0] + 1};
+}
+
+// spin precession runs for electrons (mass == m_e, particle.cpp:319) when
+// enabled and some spin is non-zero (with all spins zero it is an exact no-op)
+inline bool spin_active(const pic_ctx *c, int kind) {
+    const Species &s = c->sp[kind];
+    return c->p.spin && s.a.sx && s.spin_nonzero && c->p.mass[kind] == 1.0;
+}
+
+// kernel arguments for species `kind` of context c (host side)
+template <typename real>
+inline PushArgs<real> make_push_args(pic_ctx *c, int kind) {
+    Species &s = c->sp[kind];
+    PushArgs<real> a{};
+    a.g = c->g;
+    real **F = (real **)c->field;
+    real **R = (real **)c->ring;
+    a.ex = F[0]; a.ey = F[1]; a.ez = F[2]; a.bx = F[3]; a.by = F[4]; a.bz = F[5];
+    a.jx = R[0]; a.jy = R[1]; a.jz = R[2];
+    a.rho = c->p.deposit_rho ? R[3 + kind] : nullptr;
+    a.count = s.d_count;
+    const int cu = s.cur, nx = 1 - s.cur;
+    a.x0 = s.a.x[cu]; a.y0 = s.a.y[cu]; a.z0 = s.a.z[cu];
+    a.x1 = s.a.x[nx]; a.y1 = s.a.y[nx]; a.z1 = s.a.z[nx];
+    a.c0 = s.a.cell[cu]; a.ox0 = s.a.ox[cu]; a.oy0 = s.a.oy[cu]; a.oz0 = s.a.oz[cu];
+    a.c1 = s.a.cell[nx]; a.ox1 = s.a.ox[nx]; a.oy1 = s.a.oy[nx]; a.oz1 = s.a.oz[nx];
+    a.cp = c->cp;
+    a.px = (real *)s.a.px; a.py = (real *)s.a.py; a.pz = (real *)s.a.pz; a.w = (const real *)s.a.w;
+    a.sx = (real *)s.a.sx; a.sy = (real *)s.a.sy; a.sz = (real *)s.a.sz;
+    a.gtab = c->d_gtab; a.gtab_n = c->gtab_n;
+    const PicParams &p = c->p;
+    a.qm = (real)(p.charge[kind] / p.mass[kind] * p.dt_half);
+    a.charge = (real)p.charge[kind];
+    a.dt_d[0] = (real)(p.dt / p.dx); a.dt_d[1] = (real)(p.dt / p.dy); a.dt_d[2] = (real)(p.dt / p.dz);
+    a.dt_s = p.dt; a.dxs[0] = p.dx; a.dxs[1] = p.dy; a.dxs[2] = p.dz;
+    a.d_dt[0] = (real)(p.dx / p.dt); a.d_dt[1] = (real)(p.dy / p.dt); a.d_dt[2] = (real)(p.dz / p.dt);
+    a.E_schwinger = p.E_schwinger; a.dt_half_d = p.dt_half; a.charge_d = p.charge[kind]; a.mass_d = p.mass[kind];
+    a.electron = spin_active(c, kind) ? 1 : 0;
+    a.status = c->d_status;
+    return a;
+}
+
+}  // namespace pic

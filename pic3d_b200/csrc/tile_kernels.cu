@@ -1,0 +1,451 @@
+// Tiled gather + push + deposit with shared-memory staging.
+//
+// Particles of each species are kept in counting-sort order by cell, with
+// cells numbered tile-major (a tile is T^3 cells).  One CTA owns one tile:
+//   1. it stages the six field components of the tile plus the gather halo
+//      (T + 2H + 1 points per axis) in shared memory,
+//   2. clears shared-memory accumulators for jx, jy, jz, rho0, rho1 over the
+//      deposit footprint (T + 2H + 3 points per axis),
+//   3. pushes the particles whose sort key falls in the tile, both species,
+//      gathering from and depositing into shared memory; a particle that has
+//      left the tile since the last sort takes the global-memory path in the
+//      same loop (read-only loads, global atomics),
+//   4. flushes the accumulators with one coalesced pass of global atomics
+//      (zero entries skipped); halos of neighbouring tiles overlap, hence the
+//      atomics.
+// Lanes of a warp take particles from 32 different chunks of the tile's
+// cell-sorted list, so they sit in different cells and their shared-memory
+// addresses rarely collide.
+//
+// The counting sort (key histogram, exclusive scan, scatter into the second
+// set of arrays) runs every `sort_interval` pushes and after an upload.
+#include "pic_kernels.cuh"
+#include "push_core.cuh"
+
+namespace pic {
+
+struct TileGeom {
+    int T, nt[3];
+    long long nkeys;
+    int GE, DE, nacc;
+};
+
+template <int P>
+__host__ __device__ constexpr int gather_extent(int T) { return T + 2 * (P / 2) + 1; }
+template <int P>
+__host__ __device__ constexpr int deposit_extent(int T) { return T + 2 * (P / 2) + 3; }
+
+__device__ __forceinline__ int cell_key(const TileGeom &t, int cx, int cy, int cz) {
+    const int T = t.T;
+    int tx = cx / T, ty = cy / T, tz = cz / T;
+    int lx = cx - tx * T, ly = cy - ty * T, lz = cz - tz * T;
+    return (((tz * t.nt[1] + ty) * t.nt[0] + tx) * T + lz) * T * T + ly * T + lx;
+}
+
+// cell of a particle for sorting (FP64: periodic wrap as the next push
+// will apply it; clamped into the domain)
+__device__ __forceinline__ int particle_key(const Geom &g, const TileGeom &t, const CellPack &cp, int fp32,
+                                            const double *x, const double *y, const double *z, const int *cell,
+                                            long long i) {
+    int c[3];
+    if (fp32) {
+        cp.unpack(cell[i], c[0], c[1], c[2]);
+    } else {
+        double v[3] = {x[i], y[i], z[i]};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if (g.per[d]) {
+                if (v[d] < 0.0) v[d] += g.n[d];
+                if (v[d] > (double)g.n[d]) v[d] -= g.n[d];
+            }
+            c[d] = (int)floor(v[d]);
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) c[d] = min(max(c[d], 0), g.n[d] - 1);
+    return cell_key(t, c[0], c[1], c[2]);
+}
+
+// ---------------------------------------------------------------------------
+// counting sort
+
+struct SortArgs {
+    Geom g;
+    TileGeom t;
+    CellPack cp;
+    int fp32;
+    const long long *count;
+    const double *x, *y, *z;
+    const int *cell;
+    int *keys;
+    unsigned *hist;
+};
+
+__global__ void sort_keys_kernel(SortArgs a) {
+    long long n = *a.count;
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned act = __ballot_sync(0xffffffffu, i < n);
+    if (i >= n) return;
+    int key = particle_key(a.g, a.t, a.cp, a.fp32, a.x, a.y, a.z, a.cell, i);
+    a.keys[i] = key;
+    unsigned peers = __match_any_sync(act, key);
+    int lane = threadIdx.x & 31;
+    if (lane == __ffs(peers) - 1) atomicAdd(&a.hist[key], (unsigned)__popc(peers));
+}
+
+// exclusive scan of n unsigned values in place; block sums in `sums`
+__global__ void scan_blocks_kernel(unsigned *v, long long n, unsigned *sums) {
+    __shared__ unsigned warp_tot[32];
+    const int per = 4;
+    long long base = (long long)blockIdx.x * blockDim.x * per + (long long)threadIdx.x * per;
+    unsigned loc[per];
+    unsigned s = 0;
+#pragma unroll
+    for (int k = 0; k < per; ++k) {
+        loc[k] = base + k < n ? v[base + k] : 0u;
+        s += loc[k];
+    }
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_tot[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        int nw = blockDim.x >> 5;
+        unsigned t = lane < nw ? warp_tot[lane] : 0u;
+        unsigned ti = t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned u = __shfl_up_sync(0xffffffffu, ti, o);
+            if (lane >= o) ti += u;
+        }
+        if (lane < nw) warp_tot[lane] = ti - t;
+        if (lane == nw - 1) sums[blockIdx.x] = ti;
+    }
+    __syncthreads();
+    unsigned run = warp_tot[w] + incl - s;
+#pragma unroll
+    for (int k = 0; k < per; ++k) {
+        if (base + k < n) v[base + k] = run;
+        run += loc[k];
+    }
+}
+
+// exclusive scan of the block sums (single block, any count), total in sums[nb]
+__global__ void scan_sums_kernel(unsigned *sums, int nb) {
+    __shared__ unsigned carry;
+    __shared__ unsigned warp_tot[32];
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int off = 0; off < nb; off += blockDim.x) {
+        int i = off + threadIdx.x;
+        unsigned s = i < nb ? sums[i] : 0u;
+        int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        unsigned incl = s;
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) warp_tot[w] = incl;
+        __syncthreads();
+        if (w == 0) {
+            int nw = blockDim.x >> 5;
+            unsigned t = lane < nw ? warp_tot[lane] : 0u;
+            unsigned ti = t;
+            for (int o = 1; o < 32; o <<= 1) {
+                unsigned u = __shfl_up_sync(0xffffffffu, ti, o);
+                if (lane >= o) ti += u;
+            }
+            if (lane < nw) warp_tot[lane] = ti - t;
+        }
+        __syncthreads();
+        unsigned excl = carry + warp_tot[w] + incl - s;
+        if (i < nb) sums[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = excl + s;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) sums[nb] = carry;
+}
+
+__global__ void scan_add_kernel(unsigned *v, long long n, const unsigned *sums, int per_block, unsigned *offs_out,
+                                unsigned *cursor_out) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        unsigned o = v[i] + sums[i / per_block];
+        offs_out[i] = o;
+        cursor_out[i] = o;
+    }
+    if (i == n) {
+        int nb = (int)((n + per_block - 1) / per_block);
+        offs_out[n] = sums[nb];
+    }
+}
+
+struct ScatterArgs {
+    const long long *count;
+    long long cap;
+    unsigned *status;
+    const int *keys;
+    unsigned *cursor;
+    // up to 16 8-byte and 16 4-byte arrays moved src -> dst
+    const double *ds[16];
+    double *dd[16];
+    int nd;
+    const float *fs[16];
+    float *fd[16];
+    int nf;
+    const int *is[4];
+    int *id_[4];
+    int ni;
+};
+
+__global__ void scatter_kernel(ScatterArgs a) {
+    long long n = *a.count;
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned act = __ballot_sync(0xffffffffu, i < n);
+    if (i >= n) return;
+    int key = a.keys[i];
+    unsigned peers = __match_any_sync(act, key);
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(peers) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(&a.cursor[key], (unsigned)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    unsigned dst = base + __popc(peers & ((1u << lane) - 1u));
+    if ((long long)dst >= a.cap) {  // cannot happen with a consistent histogram; never write past the arrays
+        atomicOr(a.status, ST_OVERFLOW);
+        return;
+    }
+    for (int k = 0; k < a.nd; ++k) a.dd[k][dst] = a.ds[k][i];
+    for (int k = 0; k < a.nf; ++k) a.fd[k][dst] = a.fs[k][i];
+    for (int k = 0; k < a.ni; ++k) a.id_[k][dst] = a.is[k][i];
+}
+
+static TileGeom tile_geom(const pic_ctx *c) {
+    TileGeom t{};
+    t.T = c->tile;
+    for (int d = 0; d < 3; ++d) t.nt[d] = c->ntile[d];
+    t.nkeys = c->nkeys;
+    return t;
+}
+
+void launch_sort(pic_ctx *c, int kind) {
+    Species &s = c->sp[kind];
+    const long long n = s.n_host;
+    if (n <= 0 || c->tile <= 0) return;
+    prof_begin(c, "sort_particles");
+    const long long K = c->nkeys;
+    cudaMemsetAsync(c->d_hist, 0, (size_t)(K + 1) * sizeof(unsigned), c->stream);
+    SortArgs a{};
+    a.g = c->g;
+    a.t = tile_geom(c);
+    a.cp = c->cp;
+    a.fp32 = c->fp32;
+    a.count = s.d_count;
+    a.x = s.a.x[s.cur]; a.y = s.a.y[s.cur]; a.z = s.a.z[s.cur];
+    a.cell = s.a.cell[s.cur];
+    a.keys = s.keys;
+    a.hist = c->d_hist;
+    unsigned nb = (unsigned)((n + 255) / 256);
+    sort_keys_kernel<<<nb, 256, 0, c->stream>>>(a);
+    const int per_block = 1024 * 4;
+    int sb = (int)((K + per_block - 1) / per_block);
+    scan_blocks_kernel<<<sb, 1024, 0, c->stream>>>(c->d_hist, K, c->d_blocksums);
+    scan_sums_kernel<<<1, 1024, 0, c->stream>>>(c->d_blocksums, sb);
+    // offsets into s.offs; the cursor reuses d_hist
+    scan_add_kernel<<<(unsigned)((K + 1 + 255) / 256), 256, 0, c->stream>>>(c->d_hist, K, c->d_blocksums,
+                                                                            per_block, s.offs, c->d_hist);
+    ScatterArgs sa{};
+    sa.count = s.d_count;
+    sa.cap = s.cap;
+    sa.status = c->d_status;
+    sa.keys = s.keys;
+    sa.cursor = c->d_hist;
+    for (int b = 0; b < 2; ++b) {
+        if (c->fp32) {
+            sa.fs[sa.nf] = s.a.ox[b]; sa.fd[sa.nf++] = s.b.ox[b];
+            sa.fs[sa.nf] = s.a.oy[b]; sa.fd[sa.nf++] = s.b.oy[b];
+            sa.fs[sa.nf] = s.a.oz[b]; sa.fd[sa.nf++] = s.b.oz[b];
+            sa.is[sa.ni] = s.a.cell[b]; sa.id_[sa.ni++] = s.b.cell[b];
+        } else {
+            sa.ds[sa.nd] = s.a.x[b]; sa.dd[sa.nd++] = s.b.x[b];
+            sa.ds[sa.nd] = s.a.y[b]; sa.dd[sa.nd++] = s.b.y[b];
+            sa.ds[sa.nd] = s.a.z[b]; sa.dd[sa.nd++] = s.b.z[b];
+        }
+    }
+    void *src[7] = {s.a.px, s.a.py, s.a.pz, s.a.w, s.a.sx, s.a.sy, s.a.sz};
+    void *dst[7] = {s.b.px, s.b.py, s.b.pz, s.b.w, s.b.sx, s.b.sy, s.b.sz};
+    for (int k = 0; k < 7; ++k) {
+        if (!src[k]) continue;
+        if (c->fp32) { sa.fs[sa.nf] = (float *)src[k]; sa.fd[sa.nf++] = (float *)dst[k]; }
+        else { sa.ds[sa.nd] = (double *)src[k]; sa.dd[sa.nd++] = (double *)dst[k]; }
+    }
+    sa.is[sa.ni] = s.a.id; sa.id_[sa.ni++] = s.b.id;
+    scatter_kernel<<<nb, 256, 0, c->stream>>>(sa);
+    std::swap(s.a, s.b);
+    s.sorted = true;
+    s.pushes_since_sort = 0;
+    prof_end(c);
+}
+
+// ---------------------------------------------------------------------------
+// the tile kernel
+
+template <typename real>
+struct TileArgs {
+    PushArgs<real> sp[2];
+    const unsigned *offs[2];
+    int active[2];
+    TileGeom t;
+    real *ring[5];
+    const real *field[6];
+};
+
+template <typename real, int P, bool SPIN>
+__global__ void __launch_bounds__(256) tile_push_kernel(TileArgs<real> ta) {
+    constexpr int H = P / 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    real *sm = reinterpret_cast<real *>(smem_raw);
+    const Geom &g = ta.sp[0].g;
+    const int T = ta.t.T;
+    const int GE = gather_extent<P>(T), DE = deposit_extent<P>(T);
+    const int G2 = GE * GE, G3 = G2 * GE, D2 = DE * DE, D3 = D2 * DE;
+    real *sf = sm;
+    real *sj = sm + 6 * G3;
+    const int tile = blockIdx.x;
+    const int tx = tile % ta.t.nt[0], ty = (tile / ta.t.nt[0]) % ta.t.nt[1], tz = tile / (ta.t.nt[0] * ta.t.nt[1]);
+    const int t0[3] = {tx * T, ty * T, tz * T};
+    int gO[3], dO[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        gO[d] = t0[d] + g.mem - 1 - H;   // field buffer coordinate of the first staged point
+        dO[d] = t0[d] + g.mem - 2 - H;   // buffer coordinate of the first accumulator point
+    }
+    // 1. stage fields
+    for (int e = threadIdx.x; e < 6 * G3; e += blockDim.x) {
+        int c = e / G3, l = e - c * G3;
+        int lz = l / G2, r = l - lz * G2, ly = r / GE, lx = r - ly * GE;
+        int x = gO[0] + lx, y = gO[1] + ly, z = gO[2] + lz;
+        real v = 0;
+        if (x >= 0 && x < g.f[0] && y >= 0 && y < g.f[1] && z >= 0 && z < g.f[2]) v = __ldg(ta.field[c] + g.fi(z, y, x));
+        sf[e] = v;
+    }
+    // 2. clear accumulators
+    for (int e = threadIdx.x; e < ta.t.nacc * D3; e += blockDim.x) sj[e] = 0;
+    __syncthreads();
+
+    View<const real> fs[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) fs[c] = View<const real>{sf + c * G3, GE, G2, -(gO[2] * G2 + gO[1] * GE + gO[0])};
+    const View<real> js{sj, DE, D2, -(dO[2] * D2 + dO[1] * DE + dO[0])};
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int lo_id[3] = {t0[0] + g.mem - 1, t0[1] + g.mem - 1, t0[2] + g.mem - 1};
+
+    // 3. particles of both species
+#pragma unroll 1
+    for (int k = 0; k < 2; ++k) {
+        if (!ta.active[k]) continue;
+        const PushArgs<real> &a = ta.sp[k];
+        const long long n = *a.count;
+        const long long T3 = (long long)T * T * T;
+        long long pa = ta.offs[k][tile * T3], pb = ta.offs[k][(tile + 1) * T3];
+        pb = pb < n ? pb : n;
+        if (pa >= pb) continue;
+        const long long m = pb - pa;
+        const long long chunk = (m + 31) / 32;
+        View<const real> fg[6];
+        View<real> jg;
+        global_views(a, fg, jg);
+        real *rho_s = a.rho ? sj + (3 + k) * D3 : nullptr;
+#pragma unroll 1
+        for (long long r = warp; r < chunk; r += nwarp) {
+            const long long idx = lane * chunk + r;
+            if (idx >= m) continue;
+            const long long p = pa + idx;
+            OldPos<real> o;
+            decode_old(a, p, o);
+            bool inside = true;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) inside = inside && o.id[d] >= lo_id[d] && o.id[d] < lo_id[d] + T;
+            if (!in_buffers(g, o, H)) {
+                set_status(a.status, ST_OOB);
+            } else if (inside) {
+                push_body<real, P, SPIN, false>(a, p, o, fs, js, sj, sj + D3, sj + 2 * D3, rho_s);
+            } else {
+                push_body<real, P, SPIN, true>(a, p, o, fg, jg, a.jx, a.jy, a.jz, a.rho);
+            }
+        }
+    }
+    __syncthreads();
+    // 4. flush accumulators
+    for (int e = threadIdx.x; e < ta.t.nacc * D3; e += blockDim.x) {
+        real v = sj[e];
+        if (v == real(0)) continue;
+        int c = e / D3, l = e - c * D3;
+        int lz = l / D2, r = l - lz * D2, ly = r / DE, lx = r - ly * DE;
+        int x = dO[0] + lx, y = dO[1] + ly, z = dO[2] + lz;
+        if (x >= -1 && x <= g.f[0] && y >= -1 && y <= g.f[1] && z >= -1 && z <= g.f[2])
+            atomic_add(ta.ring[c] + g.ri(z, y, x), v);
+        else
+            set_status(ta.sp[0].status, ST_OOB);
+    }
+}
+
+size_t tile_smem_bytes(const pic_ctx *c) {
+    const int P = c->order == 2 ? 3 : 5;
+    const int T = c->tile;
+    const size_t GE = T + 2 * (P / 2) + 1, DE = T + 2 * (P / 2) + 3;
+    const size_t rs = c->fp32 ? 4 : 8;
+    return (6 * GE * GE * GE + 5 * DE * DE * DE) * rs;
+}
+
+template <typename real, int P, bool SPIN>
+static void tile_push_t(pic_ctx *c, int mask) {
+    TileArgs<real> ta{};
+    for (int k = 0; k < 2; ++k) {
+        ta.sp[k] = make_push_args<real>(c, k);
+        ta.offs[k] = c->sp[k].offs;
+        ta.active[k] = (mask >> k) & 1 && c->sp[k].n_host > 0;
+    }
+    ta.t = tile_geom(c);
+    ta.t.GE = gather_extent<P>(c->tile);
+    ta.t.DE = deposit_extent<P>(c->tile);
+    ta.t.nacc = c->p.deposit_rho ? 5 : 3;
+    for (int k = 0; k < 5; ++k) ta.ring[k] = (real *)c->ring[k];
+    for (int k = 0; k < 6; ++k) ta.field[k] = (const real *)c->field[k];
+    size_t smem = tile_smem_bytes(c);
+    cudaFuncSetAttribute(tile_push_kernel<real, P, SPIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int ntiles = c->ntile[0] * c->ntile[1] * c->ntile[2];
+    tile_push_kernel<real, P, SPIN><<<ntiles, 256, smem, c->stream>>>(ta);
+}
+
+void launch_tile_push(pic_ctx *c, int mask) {
+    for (int k = 0; k < 2; ++k) {
+        Species &s = c->sp[k];
+        if (!((mask >> k) & 1) || s.n_host <= 0) continue;
+        if (!s.sorted || s.pushes_since_sort >= c->sort_interval) launch_sort(c, k);
+    }
+    bool spin = ((mask & 1) && spin_active(c, 0)) || ((mask & 2) && spin_active(c, 1));
+    prof_begin(c, "tile_push_gather_deposit");
+    if (c->fp32) {
+        if (c->order == 2) spin ? tile_push_t<float, 3, true>(c, mask) : tile_push_t<float, 3, false>(c, mask);
+        else spin ? tile_push_t<float, 5, true>(c, mask) : tile_push_t<float, 5, false>(c, mask);
+    } else {
+        if (c->order == 2) spin ? tile_push_t<double, 3, true>(c, mask) : tile_push_t<double, 3, false>(c, mask);
+        else spin ? tile_push_t<double, 5, true>(c, mask) : tile_push_t<double, 5, false>(c, mask);
+    }
+    prof_end(c);
+    for (int k = 0; k < 2; ++k) {
+        Species &s = c->sp[k];
+        if (!((mask >> k) & 1) || s.n_host <= 0) continue;
+        s.cur = 1 - s.cur;
+        s.pushes_since_sort += 1;
+    }
+}
+
+}  // namespace pic

@@ -15,9 +15,9 @@ from parity import ARRAYS, TOL_FP32, TOL_FP64, array_errors, particle_errors, pe
 pytestmark = pytest.mark.gpu
 
 
-def _sim(params, precision="fp64", g_data=None):
+def _sim(params, precision="fp64", g_data=None, tile=0, sort_interval=0):
     from pic3d_b200.simulation import Simulation
-    s = Simulation(params, precision=precision)
+    s = Simulation(params, precision=precision, tile=tile, sort_interval=sort_interval)
     if g_data is not None:
         s.set_g_table(g_data)
     return s
@@ -28,15 +28,22 @@ def _oracle_states(g):
     return states
 
 
+# kernel paths: default shared-memory tiles, tiles sorted before every push,
+# a 2-cell tile (most particles cross tiles), and the global-memory kernel
+PATHS = {"tile4": dict(tile=0), "tile4_sort1": dict(tile=4, sort_interval=1), "tile2": dict(tile=2),
+         "global": dict(tile=-1)}
+
+
+@pytest.mark.parametrize("path", list(PATHS))
 @pytest.mark.parametrize("case", CASES)
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_teacher_forced_steps(case, precision):
+def test_teacher_forced_steps(case, precision, path):
     g = load(case)
     states = _oracle_states(g)
     tol = TOL_FP64 if precision == "fp64" else TOL_FP32
     pos_tol = 1e-11 if precision == "fp64" else 2e-6
     per = periods(g["params"])
-    sim = _sim(g["params"], precision, g["g_data"])
+    sim = _sim(g["params"], precision, g["g_data"], **PATHS[path])
     for n in range(0, g["steps"]):
         sim.upload_state(states[n])
         sim.step = n
@@ -57,12 +64,13 @@ def test_teacher_forced_steps(case, precision):
     sim.close()
 
 
+@pytest.mark.parametrize("path", ["tile4", "global"])
 @pytest.mark.parametrize("case", CASES)
-def test_free_run_fp64_matches_golden(case):
+def test_free_run_fp64_matches_golden(case, path):
     """The whole golden run (t=0 push + all steps) from the reference's
     input particles, compared with the reference's own final state."""
     g = load(case)
-    sim = _sim(g["params"], "fp64", g["g_data"])
+    sim = _sim(g["params"], "fp64", g["g_data"], **PATHS[path])
     for k in range(2):
         sim.upload_particles(k, g["input"][k])
     sim.initial_push()
