@@ -9,7 +9,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libpic3d_b200.so")
+# PIC3D_LIBRARY may point at another build of the same sources (tuning builds)
+LIB_PATH = os.environ.get("PIC3D_LIBRARY", os.path.join(HERE, "libpic3d_b200.so"))
 
 PIC_OK, PIC_EINVAL, PIC_ENOMEM, PIC_EOOB, PIC_ENAN, PIC_ETIMEOUT, PIC_ECUDA, PIC_EOVERFLOW, PIC_ERANGE = range(9)
 STATUS_NAMES = {0: "PIC_OK", 1: "PIC_EINVAL", 2: "PIC_ENOMEM", 3: "PIC_EOOB", 4: "PIC_ENAN", 5: "PIC_ETIMEOUT",

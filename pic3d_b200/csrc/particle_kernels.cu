@@ -17,8 +17,8 @@ __global__ void __launch_bounds__(256) push_kernel(PushArgs<real> a) {
     constexpr int H = P / 2;
     const long long n = *a.count;
     View<const real> fv[6];
-    View<real> jv;
-    global_views(a, fv, jv);
+    GlobalAcc<real> acc;
+    global_views(a, fv, acc);
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n;
          p += (long long)gridDim.x * blockDim.x) {
         OldPos<real> o;
@@ -27,7 +27,7 @@ __global__ void __launch_bounds__(256) push_kernel(PushArgs<real> a) {
             set_status(a.status, ST_OOB);
             continue;
         }
-        push_body<real, P, SPIN, true>(a, p, o, fv, jv, a.jx, a.jy, a.jz, a.rho);
+        push_body<real, P, SPIN, true>(a, p, o, fv, acc);
     }
 }
 

@@ -1,6 +1,7 @@
 // C ABI of libpic3d_b200.so (include/pic3d_gpu.h): context lifetime, device
 // memory, host <-> device conversion and the per-step orchestration of the
 // reference's run_main_time_loop (src/simulation.cpp:159-183).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -407,8 +408,12 @@ int pic_upload_particles(pic_ctx *c, int kind, const void *records, int64_t n) {
     const char *rec = (const char *)records;
     // every record of a species must carry the species' charge and mass
     bool spin_nonzero = false;
+    double wmax = 0.0;
     for (int64_t i = 0; i < n; ++i) {
-        double q, m, s[3];
+        double q, m, s[3], wt;
+        std::memcpy(&wt, rec + 144 * i + 128, 8);
+        if (!std::isfinite(wt)) return fail(c, PIC_EINVAL, "non-finite particle weight");
+        wmax = std::max(wmax, std::fabs(wt));
         std::memcpy(&q, rec + 144 * i + 112, 8);
         std::memcpy(&m, rec + 144 * i + 120, 8);
         if (q != c->p.charge[kind] || m != c->p.mass[kind])
@@ -425,6 +430,7 @@ int pic_upload_particles(pic_ctx *c, int kind, const void *records, int64_t n) {
     s.cur = 0;
     s.sorted = false;
     s.spin_nonzero = spin_nonzero;
+    s.max_abs_w = wmax;
     int r = ensure_stage(c, (size_t)(n < kChunk ? n : kChunk) * 144);
     if (r) return r;
     for (int64_t off = 0; off < n; off += kChunk) {

@@ -103,6 +103,7 @@ struct Species {
     unsigned *offs = nullptr;  // per-key start offsets after the last sort (nkeys + 1)
     bool sorted = false;     // offs describes the current order
     int pushes_since_sort = 0;
+    double max_abs_w = 0.0;  // largest |weight| uploaded (weights never change afterwards)
     bool spin_nonzero = false;
 };
 

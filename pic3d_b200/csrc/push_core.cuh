@@ -91,8 +91,11 @@ __device__ __forceinline__ real gather(const View<const real> &v, int i0, int j0
 // 1D pieces of the Esirkepov weights over the union span of the old and new
 // supports (src/particle.cpp:403-419): s0 = old shape, ds = new - old,
 // zero outside each support.  |i2 - i1| <= 1 (checked by the caller).
+// The weights come in FP64 whatever the working precision: ds is a
+// difference of nearly equal weights for a slow particle, and forming it in
+// FP64 keeps the FP32 path's current accurate to FP32 rounding.
 template <typename real, int P>
-__device__ __forceinline__ void span1d(int i1, const real (&w0)[P], int i2, const real (&w1)[P], int &base,
+__device__ __forceinline__ void span1d(int i1, const double (&w0)[P], int i2, const double (&w1)[P], int &base,
                                        int &len, real (&s0)[P + 1], real (&ds)[P + 1]) {
     constexpr int H = P / 2;
     const int lo = min(i1, i2);
@@ -101,32 +104,76 @@ __device__ __forceinline__ void span1d(int i1, const real (&w0)[P], int i2, cons
     const bool o0 = i1 != lo, o1 = i2 != lo;
 #pragma unroll
     for (int a = 0; a <= P; ++a) {
-        real v0 = o0 ? (a >= 1 ? w0[a - 1] : real(0)) : (a < P ? w0[a] : real(0));
-        real v1 = o1 ? (a >= 1 ? w1[a - 1] : real(0)) : (a < P ? w1[a] : real(0));
-        s0[a] = v0;
-        ds[a] = v1 - v0;
+        double v0 = o0 ? (a >= 1 ? w0[a - 1] : 0.0) : (a < P ? w0[a] : 0.0);
+        double v1 = o1 ? (a >= 1 ? w1[a - 1] : 0.0) : (a < P ? w1[a] : 0.0);
+        s0[a] = (real)v0;
+        ds[a] = (real)(v1 - v0);
     }
 }
 
 __device__ __forceinline__ void atomic_add(double *p, double v) { atomicAdd(p, v); }
 __device__ __forceinline__ void atomic_add(float *p, float v) { atomicAdd(p, v); }
 
+// Where deposited current goes.  Both accumulators address a 3D array
+// through buffer coordinates with strides (sy, sz) and offset o, like View.
+//   GlobalAcc: hardware atomics into the global ring buffers.
+//   FixedAcc:  a CTA's shared-memory tile, each value scaled to a 64-bit
+//              integer and split into 20-bit limbs added with native 32-bit
+//              integer atomics (NL = 2 limbs for FP32, 3 for FP64).  Integer
+//              sums do not depend on the order of the additions.
+template <typename real>
+struct GlobalAcc {
+    real *p[4];  // jx, jy, jz, rho (rho may be null)
+    int sy, sz, o;
+    __device__ __forceinline__ bool has_rho() const { return p[3] != nullptr; }
+    __device__ __forceinline__ void add(int c, int idx, real v) const { atomic_add(p[c] + idx, v); }
+};
+
+template <typename real, int NL>
+struct FixedAcc {
+    unsigned *p[4];   // limb 0 of jx, jy, jz, rho; limb l at + l * lstride
+    int lstride;
+    int sy, sz, o;
+    real scale[4];    // per component: value * scale is an integer below 2^(20*NL - 9) in magnitude
+    __device__ __forceinline__ bool has_rho() const { return p[3] != nullptr; }
+    __device__ __forceinline__ void add(int c, int idx, real v) const {
+        long long q;
+        if constexpr (sizeof(real) == 8) q = __double2ll_rn(v * scale[c]);
+        else q = __float2ll_rn(v * scale[c]);
+        unsigned *a = p[c] + idx;
+        atomicAdd(a, (unsigned)(q & 0xFFFFF));
+        if constexpr (NL == 2) {
+            atomicAdd(a + lstride, (unsigned)(int)(q >> 20));
+        } else {
+            atomicAdd(a + lstride, (unsigned)((q >> 20) & 0xFFFFF));
+            atomicAdd(a + 2 * lstride, (unsigned)(int)(q >> 40));
+        }
+    }
+};
+
 // Esirkepov deposit (src/particle.cpp:427-500) and rho (:503-514).  The
 // last point of each running sum (the sum of all ds, zero up to rounding)
 // is not added.
-template <typename real, int P>
-__device__ __forceinline__ void deposit(const View<real> &vj0, real *jx, real *jy, real *jz, real *rho,
-                                        const real (&dxdt)[3], const int (&i1)[3], const real (&w0)[3][P],
-                                        const int (&i2)[3], const real (&w1)[3][P], real qw) {
+template <typename real, int P, class Acc>
+__device__ __forceinline__ void deposit(const Acc &acc, const real (&dxdt)[3], const int (&i1)[3],
+                                        const double (&d0)[3], const int (&i2)[3], const double (&d1)[3],
+                                        real qw) {
     constexpr int H = P / 2;
     int base[3], len[3];
-    real s0[3][P + 1], ds[3][P + 1];
+    real s0[3][P + 1], ds[3][P + 1], w1[3][P];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) span1d<real, P>(i1[d], w0[d], i2[d], w1[d], base[d], len[d], s0[d], ds[d]);
+    for (int d = 0; d < 3; ++d) {
+        double a0[P], a1[P];
+        shape_weights(d0[d], a0);
+        shape_weights(d1[d], a1);
+        span1d<real, P>(i1[d], a0, i2[d], a1, base[d], len[d], s0[d], ds[d]);
+#pragma unroll
+        for (int q = 0; q < P; ++q) w1[d][q] = (real)a1[q];
+    }
     const real third = real(1.0 / 3.0), half = real(0.5);
     const real cx = qw * dxdt[0], cy = qw * dxdt[1], cz = qw * dxdt[2];
-    const int rx = vj0.sy, rxy = vj0.sz;
-    const int r0 = base[2] * rxy + base[1] * rx + base[0] + vj0.o;
+    const int rx = acc.sy, rxy = acc.sz;
+    const int r0 = base[2] * rxy + base[1] * rx + base[0] + acc.o;
 #pragma unroll
     for (int k = 0; k <= P; ++k) {
         if (k >= len[2]) break;
@@ -135,13 +182,13 @@ __device__ __forceinline__ void deposit(const View<real> &vj0, real *jx, real *j
             if (j >= len[1]) break;
             real wyz = s0[1][j] * s0[2][k] + half * ds[1][j] * s0[2][k] + half * s0[1][j] * ds[2][k] +
                        third * ds[1][j] * ds[2][k];
-            real acc = 0;
-            real *row = jx + r0 + k * rxy + j * rx;
+            real a = 0;
+            const int row = r0 + k * rxy + j * rx;
 #pragma unroll
             for (int i = 0; i < P; ++i) {
                 if (i >= len[0] - 1) break;
-                acc += ds[0][i];
-                atomic_add(row + i, -cx * acc * wyz);
+                a += ds[0][i];
+                acc.add(0, row + i, -cx * a * wyz);
             }
         }
     }
@@ -153,13 +200,13 @@ __device__ __forceinline__ void deposit(const View<real> &vj0, real *jx, real *j
             if (i >= len[0]) break;
             real wxz = s0[0][i] * s0[2][k] + half * ds[0][i] * s0[2][k] + half * s0[0][i] * ds[2][k] +
                        third * ds[0][i] * ds[2][k];
-            real acc = 0;
-            real *col = jy + r0 + k * rxy + i;
+            real a = 0;
+            const int col = r0 + k * rxy + i;
 #pragma unroll
             for (int j = 0; j < P; ++j) {
                 if (j >= len[1] - 1) break;
-                acc += ds[1][j];
-                atomic_add(col + j * rx, -cy * acc * wxz);
+                a += ds[1][j];
+                acc.add(1, col + j * rx, -cy * a * wxz);
             }
         }
     }
@@ -171,25 +218,25 @@ __device__ __forceinline__ void deposit(const View<real> &vj0, real *jx, real *j
             if (i >= len[0]) break;
             real wxy = s0[0][i] * s0[1][j] + half * ds[0][i] * s0[1][j] + half * s0[0][i] * ds[1][j] +
                        third * ds[0][i] * ds[1][j];
-            real acc = 0;
-            real *col = jz + r0 + j * rx + i;
+            real a = 0;
+            const int col = r0 + j * rx + i;
 #pragma unroll
             for (int k = 0; k < P; ++k) {
                 if (k >= len[2] - 1) break;
-                acc += ds[2][k];
-                atomic_add(col + k * rxy, -cz * acc * wxy);
+                a += ds[2][k];
+                acc.add(2, col + k * rxy, -cz * a * wxy);
             }
         }
     }
-    if (rho) {
-        real *rb = rho + (i2[2] - H) * rxy + (i2[1] - H) * rx + (i2[0] - H) + vj0.o;
+    if (acc.has_rho()) {
+        const int rb = (i2[2] - H) * rxy + (i2[1] - H) * rx + (i2[0] - H) + acc.o;
 #pragma unroll
         for (int k = 0; k < P; ++k)
 #pragma unroll
             for (int j = 0; j < P; ++j) {
                 real wjk = qw * w1[1][j] * w1[2][k];
 #pragma unroll
-                for (int i = 0; i < P; ++i) atomic_add(rb + k * rxy + j * rx + i, wjk * w1[0][i]);
+                for (int i = 0; i < P; ++i) acc.add(3, rb + k * rxy + j * rx + i, wjk * w1[0][i]);
             }
     }
 }
@@ -255,10 +302,9 @@ __device__ __forceinline__ void decode_old(const PushArgs<real> &a, long long p,
 // Everything after the position decode: gather, Boris, move, deposit,
 // store, spin.  fv: the six field views; jv: view for the current arrays
 // (jx..rho share its strides).
-template <typename real, int P, bool SPIN, bool LDG>
+template <typename real, int P, bool SPIN, bool LDG, class Acc>
 __device__ __forceinline__ void push_body(const PushArgs<real> &a, long long p, const OldPos<real> &o,
-                                          const View<const real> (&fv)[6], const View<real> &jv, real *jx,
-                                          real *jy, real *jz, real *rho) {
+                                          const View<const real> (&fv)[6], const Acc &acc) {
     constexpr bool F64 = cuda::std::is_same<real, double>::value;
     constexpr int H = P / 2;
     const Geom &g = a.g;
@@ -294,7 +340,7 @@ __device__ __forceinline__ void push_body(const PushArgs<real> &a, long long p, 
     real gam = sqrt(real(1) + (pxn * pxn + pyn * pyn + pzn * pzn));
     // move in cell units (particle.cpp:313-315)
     int i2[3];
-    real d2[3];
+    double d0[3], d2[3];   // primal offsets of the old and new position for the deposit (FP64)
     double xn[3];
     int cn[3];
     real on[3];
@@ -307,11 +353,13 @@ __device__ __forceinline__ void push_body(const PushArgs<real> &a, long long p, 
             double xc = xn[d] - (double)(1 - g.mem);
             i2[d] = (int)(xc + 0.5);
             d2[d] = xc - (double)i2[d];
+            d0[d] = o.dp[d];
         }
     } else {
         const real disp[3] = {pxn / gam * a.dt_d[0], pyn / gam * a.dt_d[1], pzn / gam * a.dt_d[2]};
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
+            // stored position: cell + FP32 offset in [0, 1)
             real q = o.oo[d] + disp[d];
             int s = 0;
             if (q >= real(1)) { q -= real(1); s = 1; }
@@ -322,10 +370,12 @@ __device__ __forceinline__ void push_body(const PushArgs<real> &a, long long p, 
             }
             cn[d] = o.cc[d] + s;
             on[d] = q;
-            int b = cn[d] + g.mem - 1;
-            bool up = q >= real(0.5);
-            i2[d] = b + (up ? 1 : 0);
-            d2[d] = up ? q - real(1) : q;
+            // deposit: the unrounded move old offset + displacement, in FP64
+            double u = (double)o.oo[d] + (double)disp[d];
+            double f = floor(u + 0.5);
+            i2[d] = o.cc[d] + g.mem - 1 + (int)f;
+            d2[d] = u - f;
+            d0[d] = (double)o.dp[d];
         }
     }
     bool fin = isfinite(pxn) && isfinite(pyn) && isfinite(pzn);
@@ -334,11 +384,8 @@ __device__ __forceinline__ void push_body(const PushArgs<real> &a, long long p, 
         set_status(a.status, fin ? ST_CFL : ST_NAN);
         return;
     }
-    real w1[3][P];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) shape_weights(d2[d], w1[d]);
     const real qw = a.charge * a.w[p];
-    deposit<real, P>(jv, jx, jy, jz, rho, a.d_dt, o.ip, wp, i2, w1, qw);
+    deposit<real, P>(acc, a.d_dt, o.ip, d0, i2, d2, qw);
     // store
     a.px[p] = pxn;
     a.py[p] = pyn;
@@ -402,12 +449,13 @@ __device__ __forceinline__ bool in_buffers(const Geom &g, const OldPos<real> &o,
 }
 
 template <typename real>
-__device__ __forceinline__ void global_views(const PushArgs<real> &a, View<const real> (&fv)[6], View<real> &jv) {
+__device__ __forceinline__ void global_views(const PushArgs<real> &a, View<const real> (&fv)[6],
+                                             GlobalAcc<real> &acc) {
     const Geom &g = a.g;
     const real *f[6] = {a.ex, a.ey, a.ez, a.bx, a.by, a.bz};
 #pragma unroll
     for (int c = 0; c < 6; ++c) fv[c] = View<const real>{f[c], g.f[0], g.fxy, 0};
-    jv = View<real>{a.jx, g.r[0], g.rxy, g.rxy + g.r[0] + 1};
+    acc = GlobalAcc<real>{{a.jx, a.jy, a.jz, a.rho}, g.r[0], g.rxy, g.rxy + g.r[0] + 1};
 }
 
 // spin precession runs for electrons (mass == m_e, particle.cpp:319) when

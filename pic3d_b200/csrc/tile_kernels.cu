@@ -19,6 +19,9 @@
 //
 // The counting sort (key histogram, exclusive scan, scatter into the second
 // set of arrays) runs every `sort_interval` pushes and after an upload.
+#include <algorithm>
+#include <cmath>
+
 #include "pic_kernels.cuh"
 #include "push_core.cuh"
 
@@ -296,6 +299,14 @@ void launch_sort(pic_ctx *c, int kind) {
 // ---------------------------------------------------------------------------
 // the tile kernel
 
+// limbs of the shared-memory fixed-point accumulators
+template <typename real>
+constexpr int limbs() { return sizeof(real) == 8 ? 3 : 2; }
+// |value * scale| stays below 2^(20*NL - 9): with at most kMaxTileParticles
+// additions per point the 20-bit limb sums fit in 32 bits and the
+// reassembled total in 64 bits
+constexpr int kMaxTileParticles = 4095;
+
 template <typename real>
 struct TileArgs {
     PushArgs<real> sp[2];
@@ -304,19 +315,26 @@ struct TileArgs {
     TileGeom t;
     real *ring[5];
     const real *field[6];
+    real scale[4];          // jx, jy, jz, rho
+    double inv_scale[4];
 };
 
+#ifndef PIC_TILE_MIN_BLOCKS
+#define PIC_TILE_MIN_BLOCKS 1
+#endif
+
 template <typename real, int P, bool SPIN>
-__global__ void __launch_bounds__(256) tile_push_kernel(TileArgs<real> ta) {
+__global__ void __launch_bounds__(256, PIC_TILE_MIN_BLOCKS) tile_push_kernel(TileArgs<real> ta) {
     constexpr int H = P / 2;
+    constexpr int NL = limbs<real>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    real *sm = reinterpret_cast<real *>(smem_raw);
+    real *sf = reinterpret_cast<real *>(smem_raw);
     const Geom &g = ta.sp[0].g;
     const int T = ta.t.T;
     const int GE = gather_extent<P>(T), DE = deposit_extent<P>(T);
     const int G2 = GE * GE, G3 = G2 * GE, D2 = DE * DE, D3 = D2 * DE;
-    real *sf = sm;
-    real *sj = sm + 6 * G3;
+    unsigned *sa = reinterpret_cast<unsigned *>(sf + 6 * G3);   // [component][limb][D3]
+    const int nacc = ta.t.nacc;
     const int tile = blockIdx.x;
     const int tx = tile % ta.t.nt[0], ty = (tile / ta.t.nt[0]) % ta.t.nt[1], tz = tile / (ta.t.nt[0] * ta.t.nt[1]);
     const int t0[3] = {tx * T, ty * T, tz * T};
@@ -326,69 +344,95 @@ __global__ void __launch_bounds__(256) tile_push_kernel(TileArgs<real> ta) {
         gO[d] = t0[d] + g.mem - 1 - H;   // field buffer coordinate of the first staged point
         dO[d] = t0[d] + g.mem - 2 - H;   // buffer coordinate of the first accumulator point
     }
-    // 1. stage fields
-    for (int e = threadIdx.x; e < 6 * G3; e += blockDim.x) {
-        int c = e / G3, l = e - c * G3;
-        int lz = l / G2, r = l - lz * G2, ly = r / GE, lx = r - ly * GE;
-        int x = gO[0] + lx, y = gO[1] + ly, z = gO[2] + lz;
-        real v = 0;
-        if (x >= 0 && x < g.f[0] && y >= 0 && y < g.f[1] && z >= 0 && z < g.f[2]) v = __ldg(ta.field[c] + g.fi(z, y, x));
-        sf[e] = v;
+    // particle ranges of this tile
+    const long long T3 = (long long)T * T * T;
+    long long pa[2] = {0, 0}, pb[2] = {0, 0};
+    long long mtot = 0;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        if (!ta.active[k]) continue;
+        const long long n = *ta.sp[k].count;
+        pa[k] = ta.offs[k][tile * T3];
+        pb[k] = ta.offs[k][(tile + 1) * T3];
+        pb[k] = pb[k] < n ? pb[k] : n;
+        if (pa[k] > pb[k]) pa[k] = pb[k];
+        mtot += pb[k] - pa[k];
     }
-    // 2. clear accumulators
-    for (int e = threadIdx.x; e < ta.t.nacc * D3; e += blockDim.x) sj[e] = 0;
+    if (mtot == 0) return;
+    const bool use_smem = mtot <= kMaxTileParticles;
+    // 1. stage fields, 2. clear accumulators
+    if (use_smem) {
+        for (int e = threadIdx.x; e < 6 * G3; e += blockDim.x) {
+            int c = e / G3, l = e - c * G3;
+            int lz = l / G2, r = l - lz * G2, ly = r / GE, lx = r - ly * GE;
+            int x = gO[0] + lx, y = gO[1] + ly, z = gO[2] + lz;
+            real v = 0;
+            if (x >= 0 && x < g.f[0] && y >= 0 && y < g.f[1] && z >= 0 && z < g.f[2])
+                v = __ldg(ta.field[c] + g.fi(z, y, x));
+            sf[e] = v;
+        }
+        for (int e = threadIdx.x; e < nacc * NL * D3; e += blockDim.x) sa[e] = 0u;
+    }
     __syncthreads();
 
     View<const real> fs[6];
 #pragma unroll
     for (int c = 0; c < 6; ++c) fs[c] = View<const real>{sf + c * G3, GE, G2, -(gO[2] * G2 + gO[1] * GE + gO[0])};
-    const View<real> js{sj, DE, D2, -(dO[2] * D2 + dO[1] * DE + dO[0])};
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     const int lo_id[3] = {t0[0] + g.mem - 1, t0[1] + g.mem - 1, t0[2] + g.mem - 1};
 
     // 3. particles of both species
 #pragma unroll 1
     for (int k = 0; k < 2; ++k) {
-        if (!ta.active[k]) continue;
+        if (pb[k] <= pa[k]) continue;
         const PushArgs<real> &a = ta.sp[k];
-        const long long n = *a.count;
-        const long long T3 = (long long)T * T * T;
-        long long pa = ta.offs[k][tile * T3], pb = ta.offs[k][(tile + 1) * T3];
-        pb = pb < n ? pb : n;
-        if (pa >= pb) continue;
-        const long long m = pb - pa;
+        const long long m = pb[k] - pa[k];
         const long long chunk = (m + 31) / 32;
         View<const real> fg[6];
-        View<real> jg;
-        global_views(a, fg, jg);
-        real *rho_s = a.rho ? sj + (3 + k) * D3 : nullptr;
+        GlobalAcc<real> ag;
+        global_views(a, fg, ag);
+        FixedAcc<real, NL> af;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) af.p[c] = sa + c * NL * D3;
+        af.p[3] = (a.rho && nacc == 5) ? sa + (3 + k) * NL * D3 : nullptr;
+        af.lstride = D3;
+        af.sy = DE;
+        af.sz = D2;
+        af.o = -(dO[2] * D2 + dO[1] * DE + dO[0]);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) af.scale[c] = ta.scale[c];
 #pragma unroll 1
         for (long long r = warp; r < chunk; r += nwarp) {
             const long long idx = lane * chunk + r;
             if (idx >= m) continue;
-            const long long p = pa + idx;
+            const long long p = pa[k] + idx;
             OldPos<real> o;
             decode_old(a, p, o);
-            bool inside = true;
+            bool inside = use_smem;
 #pragma unroll
             for (int d = 0; d < 3; ++d) inside = inside && o.id[d] >= lo_id[d] && o.id[d] < lo_id[d] + T;
             if (!in_buffers(g, o, H)) {
                 set_status(a.status, ST_OOB);
             } else if (inside) {
-                push_body<real, P, SPIN, false>(a, p, o, fs, js, sj, sj + D3, sj + 2 * D3, rho_s);
+                push_body<real, P, SPIN, false>(a, p, o, fs, af);
             } else {
-                push_body<real, P, SPIN, true>(a, p, o, fg, jg, a.jx, a.jy, a.jz, a.rho);
+                push_body<real, P, SPIN, true>(a, p, o, fg, ag);
             }
         }
     }
+    if (!use_smem) return;
     __syncthreads();
-    // 4. flush accumulators
-    for (int e = threadIdx.x; e < ta.t.nacc * D3; e += blockDim.x) {
-        real v = sj[e];
-        if (v == real(0)) continue;
+    // 4. reassemble the limbs and flush with one pass of global atomics
+    for (int e = threadIdx.x; e < nacc * D3; e += blockDim.x) {
         int c = e / D3, l = e - c * D3;
+        const unsigned *q = sa + c * NL * D3 + l;
+        long long tot;
+        if constexpr (NL == 2) tot = ((long long)(int)q[D3] << 20) + (long long)q[0];
+        else tot = ((long long)(int)q[2 * D3] << 40) + ((long long)q[D3] << 20) + (long long)q[0];
+        if (tot == 0) continue;
         int lz = l / D2, r = l - lz * D2, ly = r / DE, lx = r - ly * DE;
         int x = dO[0] + lx, y = dO[1] + ly, z = dO[2] + lz;
+        const real v = (real)((double)tot * ta.inv_scale[c < 3 ? c : 3]);
         if (x >= -1 && x <= g.f[0] && y >= -1 && y <= g.f[1] && z >= -1 && z <= g.f[2])
             atomic_add(ta.ring[c] + g.ri(z, y, x), v);
         else
@@ -400,17 +444,19 @@ size_t tile_smem_bytes(const pic_ctx *c) {
     const int P = c->order == 2 ? 3 : 5;
     const int T = c->tile;
     const size_t GE = T + 2 * (P / 2) + 1, DE = T + 2 * (P / 2) + 3;
-    const size_t rs = c->fp32 ? 4 : 8;
-    return (6 * GE * GE * GE + 5 * DE * DE * DE) * rs;
+    const size_t rs = c->fp32 ? 4 : 8, nl = c->fp32 ? 2 : 3;
+    return 6 * GE * GE * GE * rs + 5 * nl * DE * DE * DE * 4;
 }
 
 template <typename real, int P, bool SPIN>
 static void tile_push_t(pic_ctx *c, int mask) {
     TileArgs<real> ta{};
+    double qw_max = 0.0;
     for (int k = 0; k < 2; ++k) {
         ta.sp[k] = make_push_args<real>(c, k);
         ta.offs[k] = c->sp[k].offs;
-        ta.active[k] = (mask >> k) & 1 && c->sp[k].n_host > 0;
+        ta.active[k] = ((mask >> k) & 1) && c->sp[k].n_host > 0;
+        if (ta.active[k]) qw_max = std::max(qw_max, std::fabs(c->p.charge[k]) * c->sp[k].max_abs_w);
     }
     ta.t = tile_geom(c);
     ta.t.GE = gather_extent<P>(c->tile);
@@ -418,6 +464,17 @@ static void tile_push_t(pic_ctx *c, int mask) {
     ta.t.nacc = c->p.deposit_rho ? 5 : 3;
     for (int k = 0; k < 5; ++k) ta.ring[k] = (real *)c->ring[k];
     for (int k = 0; k < 6; ++k) ta.field[k] = (const real *)c->field[k];
+    // one contribution is at most |q w| d/dt (J: the running sum of ds and the
+    // Esirkepov weight are both within [-1, 1]) or |q w| (rho)
+    const double dmax = std::max(c->p.dx, std::max(c->p.dy, c->p.dz));
+    const double lim = std::ldexp(1.0, 20 * limbs<real>() - 9);
+    const double bj = 1.01 * qw_max * dmax / c->p.dt, br = 1.01 * qw_max;
+    for (int k = 0; k < 4; ++k) {
+        double b = k < 3 ? bj : br;
+        double s = b > 0.0 ? lim / b : 1.0;
+        ta.scale[k] = (real)s;
+        ta.inv_scale[k] = 1.0 / (double)ta.scale[k];
+    }
     size_t smem = tile_smem_bytes(c);
     cudaFuncSetAttribute(tile_push_kernel<real, P, SPIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int ntiles = c->ntile[0] * c->ntile[1] * c->ntile[2];
