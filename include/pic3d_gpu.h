@@ -149,6 +149,25 @@ int pic_get_stream(const pic_ctx *ctx, void **stream);
 #define PIC_NDIAG 6
 int pic_diagnostics(pic_ctx *ctx, double *out, int n);
 
+/* ---- diagnostics without device allocation (no reference counterpart) --
+ * For callers that cannot let a library call cudaMalloc (a host code that
+ * reserves nearly all of HBM for its own arrays, or that allows device
+ * memory only through its own pool; cudaMalloc / cudaFree would fail or
+ * synchronise the device).  Needs no context: reads caller-owned FP64 device
+ * arrays in the reference layout (rho0 / rho1 may be NULL) for the grid that
+ * p->local_*cells, p->mem and p->dx.. describe, and writes 4 doubles to the
+ * caller-owned device array `out`, stream-ordered on `stream`:
+ * out[0] field energy, out[1] charge of species 0, out[2] charge of species 1,
+ * out[3] max |div E - rho0 - rho1| — the same quantities as pic_diagnostics
+ * out[0], out[3], out[4], out[5].  Its only scratch is a static device array
+ * of one slot per z plane: grids with more than 2048 z planes are rejected
+ * with PIC_EINVAL.  The first call on each device looks up that array's
+ * address (no allocation); make it before capturing work on the device into
+ * a stream.  All calls share the array: calls that overlap on the GPU race. */
+int pic_field_diagnostics_noalloc(const PicParams *p, const double *ex, const double *ey, const double *ez,
+                                  const double *bx, const double *by, const double *bz, const double *rho0,
+                                  const double *rho1, double *out, void *stream);
+
 /* ---- per-kernel timing with CUDA events (off by default) ------------- */
 int pic_profile_enable(pic_ctx *ctx, int on);
 /* names[i] (static strings), total_ms[i] and launches[i] for up to cap kernels */

@@ -52,7 +52,7 @@ EXPORTS = [
     "pic_update_fields_second", "pic_clear_currents", "pic_update_particles", "pic_exchange_particles",
     "pic_exchange_currents", "pic_initial_push", "pic_run_steps", "pic_get_step", "pic_set_step",
     "pic_synchronize", "pic_get_stream", "pic_diagnostics", "pic_profile_enable", "pic_profile_read",
-    "pic_profile_reset", "pic_save", "pic_load",
+    "pic_profile_reset", "pic_save", "pic_load", "pic_field_diagnostics_noalloc",
 ]
 
 
@@ -92,6 +92,7 @@ def load(path: str = LIB_PATH):
     lib.pic_diagnostics.argtypes = [V, V, ctypes.c_int]
     lib.pic_profile_enable.argtypes = [V, ctypes.c_int]
     lib.pic_profile_read.argtypes = [V, P(ctypes.c_char_p), P(_D), P(_I64), ctypes.c_int, P(ctypes.c_int)]
+    lib.pic_field_diagnostics_noalloc.argtypes = [P(PicParams)] + [V] * 10
     lib.pic_save.argtypes = [V, ctypes.c_char_p]
     lib.pic_load.argtypes = [V, ctypes.c_char_p]
     _lib = lib
