@@ -19,8 +19,9 @@ __global__ void __launch_bounds__(256) push_kernel(PushArgs<real> a) {
     View<const real> fv[6];
     GlobalAcc<real> acc;
     global_views(a, fv, acc);
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n;
-         p += (long long)gridDim.x * blockDim.x) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long p = a.idx ? (long long)a.idx[t] : t;
         OldPos<real> o;
         decode_old(a, p, o);
         if (!in_buffers(a.g, o, H)) {
@@ -52,8 +53,34 @@ static void push_t(pic_ctx *c, int kind) {
     s.cur = 1 - s.cur;
 }
 
-void launch_push(pic_ctx *c, int kind) {
+// the particles listed in idx (count on the device), e.g. those the tiled
+// kernel left because they moved out of their tile since the last sort
+template <typename real, int P, bool SPIN>
+static void push_list_t(pic_ctx *c, int kind, const int *idx, const unsigned long long *count) {
     Species &s = c->sp[kind];
+    PushArgs<real> a = make_push_args<real>(c, kind);
+    a.idx = idx;
+    a.count = reinterpret_cast<const long long *>(count);
+    long long n = s.n_host;
+    if (n > 0) {
+        long long blocks = (n + 255) / 256;
+        long long maxb = (long long)sm_count(c) * 4;
+        push_kernel<real, P, SPIN><<<(unsigned)(blocks < maxb ? blocks : maxb), 256, 0, c->stream>>>(a);
+    }
+}
+
+void launch_push_list(pic_ctx *c, int kind, const int *idx, const unsigned long long *count) {
+    bool spin = spin_active(c, kind);
+    if (c->fp32) {
+        if (c->order == 2) spin ? push_list_t<float, 3, true>(c, kind, idx, count) : push_list_t<float, 3, false>(c, kind, idx, count);
+        else spin ? push_list_t<float, 5, true>(c, kind, idx, count) : push_list_t<float, 5, false>(c, kind, idx, count);
+    } else {
+        if (c->order == 2) spin ? push_list_t<double, 3, true>(c, kind, idx, count) : push_list_t<double, 3, false>(c, kind, idx, count);
+        else spin ? push_list_t<double, 5, true>(c, kind, idx, count) : push_list_t<double, 5, false>(c, kind, idx, count);
+    }
+}
+
+void launch_push(pic_ctx *c, int kind) {
     bool spin = spin_active(c, kind);
     prof_begin(c, "push_gather_deposit");
     if (c->fp32) {

@@ -66,6 +66,7 @@ void free_species(Species &s) {
     free_arrays(s.b);
     if (s.d_count) cudaFree(s.d_count);
     if (s.keys) cudaFree(s.keys);
+    if (s.strag) cudaFree(s.strag);
     if (s.offs) cudaFree(s.offs);
     s = Species{};
 }
@@ -104,6 +105,7 @@ int alloc_species(pic_ctx *c, int kind, int64_t cap, bool spin) {
     if (c->tile > 0 && cap > 0) {
         r = r ? r : alloc_arrays(c, s.b, n, spin);
         r = r ? r : dalloc(c, &s.keys, n * sizeof(int));
+        r = r ? r : dalloc(c, &s.strag, n * sizeof(int));
         r = r ? r : dalloc(c, &s.offs, (size_t)(c->nkeys + 1) * sizeof(unsigned));
     }
     r = r ? r : dalloc(c, &s.d_count, sizeof(long long));
@@ -307,6 +309,7 @@ int pic_create(const PicParams *pp, int device, pic_ctx **out) {
     if (c->tile > 0) {
         r = r ? r : dalloc(c, &c->d_hist, (size_t)(c->nkeys + 1) * sizeof(unsigned));
         r = r ? r : dalloc(c, &c->d_blocksums, (size_t)(c->nkeys / 4096 + 2) * sizeof(unsigned));
+        r = r ? r : dalloc(c, &c->d_nstrag, 2 * sizeof(unsigned long long));
     }
     if (r != PIC_OK) {
         std::fprintf(stderr, "pic_create: %s\n", c->err.c_str());
@@ -346,7 +349,7 @@ int pic_destroy(pic_ctx *c) {
         if (p) cudaFree(p);
     for (auto &s : c->sp) free_species(s);
     void *ptrs[] = {c->d_status, c->d_gtab, c->d_profile, c->d_stage, c->d_scratch_ll, c->d_list, c->d_diag,
-                    c->d_hist, c->d_blocksums};
+                    c->d_hist, c->d_blocksums, c->d_nstrag};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);

@@ -100,6 +100,7 @@ struct Species {
     PartArrays a;            // the particles
     PartArrays b;            // destination of the counting sort (same shapes)
     int *keys = nullptr;     // per-particle sort key
+    int *strag = nullptr;    // particles the tiled kernel hands to the global kernel
     unsigned *offs = nullptr;  // per-key start offsets after the last sort (nkeys + 1)
     bool sorted = false;     // offs describes the current order
     int pushes_since_sort = 0;
@@ -159,6 +160,7 @@ struct pic_ctx {
     long long nkeys = 0;                 // ntiles * tile^3
     unsigned *d_hist = nullptr;          // nkeys + 1
     unsigned *d_blocksums = nullptr;
+    unsigned long long *d_nstrag = nullptr;   // straggler counts, one per species
     int sort_interval = 4;
     int steps_since_sort = 0;
     int step = 0;

@@ -17,6 +17,7 @@ void launch_radiating_boundary(pic_ctx *c, int is_left, int is_right, int step);
 
 // particle_kernels.cu
 void launch_push(pic_ctx *c, int kind);
+void launch_push_list(pic_ctx *c, int kind, const int *idx, const unsigned long long *count);
 void launch_remove(pic_ctx *c, int kind);
 void launch_upload_particles(pic_ctx *c, int kind, const void *d_records, int64_t n, int64_t offset);
 void launch_download_particles(pic_ctx *c, int kind, void *d_records, int64_t n, int64_t offset);

@@ -17,6 +17,7 @@ struct PushArgs {
     const real *ex, *ey, *ez, *bx, *by, *bz;
     real *jx, *jy, *jz, *rho;
     const long long *count;
+    const int *idx;          // optional list of particle indices (count entries); null: all particles
     // FP64 positions (cur -> nxt)
     double *x0, *y0, *z0;
     double *x1, *y1, *z1;
@@ -52,6 +53,17 @@ struct View {
 
 __device__ __forceinline__ void set_status(unsigned *s, unsigned bit) { atomicOr(s, bit); }
 
+// a[i] for a register array and a run-time index, as a chain of selects
+// (keeps `a` in registers; used where an outer stencil loop stays rolled to
+// keep the kernel's code small enough for the instruction cache)
+template <typename T, int N>
+__device__ __forceinline__ T pick(const T (&a)[N], int i) {
+    T v = a[0];
+#pragma unroll
+    for (int q = 1; q < N; ++q) v = (i == q) ? a[q] : v;
+    return v;
+}
+
 // g_factor lookup (src/particle.cpp:603-637)
 __device__ __forceinline__ double g_factor_dev(const double *tab, int n, double x, unsigned *status) {
     int idx;
@@ -72,7 +84,7 @@ __device__ __forceinline__ real gather(const View<const real> &v, int i0, int j0
                                        const real (&wy)[P], const real (&wz)[P]) {
     const real *base = v.at(k0, j0, i0);
     real acc = 0;
-#pragma unroll
+#pragma unroll 1
     for (int k = 0; k < P; ++k) {
         real acck = 0;
 #pragma unroll
@@ -83,7 +95,7 @@ __device__ __forceinline__ real gather(const View<const real> &v, int i0, int j0
             for (int i = 0; i < P; ++i) s += wx[i] * (LDG ? __ldg(row + i) : row[i]);
             acck += wy[j] * s;
         }
-        acc += wz[k] * acck;
+        acc += pick(wz, k) * acck;
     }
     return acc;
 }
@@ -134,19 +146,31 @@ struct FixedAcc {
     unsigned *p[4];   // limb 0 of jx, jy, jz, rho; limb l at + l * lstride
     int lstride;
     int sy, sz, o;
-    real scale[4];    // per component: value * scale is an integer below 2^(20*NL - 9) in magnitude
+    real scale[4];    // per component: |value * scale| < 2^(20*NL - 9)
     __device__ __forceinline__ bool has_rho() const { return p[3] != nullptr; }
+    // Exact round-to-nearest of the scaled value by the add-a-magic-constant
+    // method (the sum's low mantissa bits are the integer), split into
+    // signed limbs: FP64 q = l2*2^40 + l1*2^20 + l0 with l0, l1 in [0, 2^20);
+    // FP32 q = h*2^20 + l with |l| <= 2^19.  Adding zero is skipped.
     __device__ __forceinline__ void add(int c, int idx, real v) const {
-        long long q;
-        if constexpr (sizeof(real) == 8) q = __double2ll_rn(v * scale[c]);
-        else q = __float2ll_rn(v * scale[c]);
+        if (v == real(0)) return;
         unsigned *a = p[c] + idx;
-        atomicAdd(a, (unsigned)(q & 0xFFFFF));
-        if constexpr (NL == 2) {
-            atomicAdd(a + lstride, (unsigned)(int)(q >> 20));
+        if constexpr (NL == 3) {
+            const double q = (double)v * (double)scale[c];               // |q| < 2^51
+            const long long qi = __double_as_longlong(q + 6755399441055744.0) - 0x4338000000000000LL;
+            atomicAdd(a, (unsigned)(qi & 0xFFFFF));
+            atomicAdd(a + lstride, (unsigned)((qi >> 20) & 0xFFFFF));
+            atomicAdd(a + 2 * lstride, (unsigned)(int)(qi >> 40));
         } else {
-            atomicAdd(a + lstride, (unsigned)((q >> 20) & 0xFFFFF));
-            atomicAdd(a + 2 * lstride, (unsigned)(int)(q >> 40));
+            const float q = (float)v * (float)scale[c];                  // |q| < 2^31
+            const float magic = 12582912.0f;                             // 1.5 * 2^23
+            const float t = fmaf(q, 1.0f / 1048576.0f, magic);           // round(q / 2^20) + magic
+            const float h = t - magic;
+            const float lo = fmaf(-h, 1048576.0f, q);                     // exact, |lo| <= 2^19
+            const int li = __float_as_int(lo + magic) - 0x4B400000;
+            const int hi = __float_as_int(t) - 0x4B400000;
+            atomicAdd(a, (unsigned)li);
+            atomicAdd(a + lstride, (unsigned)hi);
         }
     }
 };
@@ -174,14 +198,14 @@ __device__ __forceinline__ void deposit(const Acc &acc, const real (&dxdt)[3], c
     const real cx = qw * dxdt[0], cy = qw * dxdt[1], cz = qw * dxdt[2];
     const int rx = acc.sy, rxy = acc.sz;
     const int r0 = base[2] * rxy + base[1] * rx + base[0] + acc.o;
-#pragma unroll
-    for (int k = 0; k <= P; ++k) {
-        if (k >= len[2]) break;
+    // Jx: running sum of ds along x times the yz weight
+#pragma unroll 1
+    for (int k = 0; k < len[2]; ++k) {
+        const real s0z = pick(s0[2], k), dsz = pick(ds[2], k);
 #pragma unroll
         for (int j = 0; j <= P; ++j) {
             if (j >= len[1]) break;
-            real wyz = s0[1][j] * s0[2][k] + half * ds[1][j] * s0[2][k] + half * s0[1][j] * ds[2][k] +
-                       third * ds[1][j] * ds[2][k];
+            real wyz = s0[1][j] * s0z + half * ds[1][j] * s0z + half * s0[1][j] * dsz + third * ds[1][j] * dsz;
             real a = 0;
             const int row = r0 + k * rxy + j * rx;
 #pragma unroll
@@ -192,14 +216,14 @@ __device__ __forceinline__ void deposit(const Acc &acc, const real (&dxdt)[3], c
             }
         }
     }
-#pragma unroll
-    for (int k = 0; k <= P; ++k) {
-        if (k >= len[2]) break;
+    // Jy
+#pragma unroll 1
+    for (int k = 0; k < len[2]; ++k) {
+        const real s0z = pick(s0[2], k), dsz = pick(ds[2], k);
 #pragma unroll
         for (int i = 0; i <= P; ++i) {
             if (i >= len[0]) break;
-            real wxz = s0[0][i] * s0[2][k] + half * ds[0][i] * s0[2][k] + half * s0[0][i] * ds[2][k] +
-                       third * ds[0][i] * ds[2][k];
+            real wxz = s0[0][i] * s0z + half * ds[0][i] * s0z + half * s0[0][i] * dsz + third * ds[0][i] * dsz;
             real a = 0;
             const int col = r0 + k * rxy + i;
 #pragma unroll
@@ -210,14 +234,14 @@ __device__ __forceinline__ void deposit(const Acc &acc, const real (&dxdt)[3], c
             }
         }
     }
-#pragma unroll
-    for (int j = 0; j <= P; ++j) {
-        if (j >= len[1]) break;
+    // Jz
+#pragma unroll 1
+    for (int j = 0; j < len[1]; ++j) {
+        const real s0y = pick(s0[1], j), dsy = pick(ds[1], j);
 #pragma unroll
         for (int i = 0; i <= P; ++i) {
             if (i >= len[0]) break;
-            real wxy = s0[0][i] * s0[1][j] + half * ds[0][i] * s0[1][j] + half * s0[0][i] * ds[1][j] +
-                       third * ds[0][i] * ds[1][j];
+            real wxy = s0[0][i] * s0y + half * ds[0][i] * s0y + half * s0[0][i] * dsy + third * ds[0][i] * dsy;
             real a = 0;
             const int col = r0 + j * rx + i;
 #pragma unroll
@@ -230,14 +254,16 @@ __device__ __forceinline__ void deposit(const Acc &acc, const real (&dxdt)[3], c
     }
     if (acc.has_rho()) {
         const int rb = (i2[2] - H) * rxy + (i2[1] - H) * rx + (i2[0] - H) + acc.o;
-#pragma unroll
-        for (int k = 0; k < P; ++k)
+#pragma unroll 1
+        for (int k = 0; k < P; ++k) {
+            const real wk = qw * pick(w1[2], k);
 #pragma unroll
             for (int j = 0; j < P; ++j) {
-                real wjk = qw * w1[1][j] * w1[2][k];
+                real wjk = wk * w1[1][j];
 #pragma unroll
                 for (int i = 0; i < P; ++i) acc.add(3, rb + k * rxy + j * rx + i, wjk * w1[0][i]);
             }
+        }
     }
 }
 

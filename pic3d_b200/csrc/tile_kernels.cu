@@ -31,7 +31,22 @@ struct TileGeom {
     int T, nt[3];
     long long nkeys;
     int GE, DE, nacc;
+    // padded shared-memory strides: row gsy/dsy, plane gsz/dsz, array gsize/dsize
+    int gsy, gsz, gsize, dsy, dsz, dsize;
 };
+
+// Row and plane strides of a shared-memory box of extent e for tile edge T.
+// Lanes of a warp take 32 consecutive cells of the tile (cell index
+// x + T*y + T*T*z); with row stride = T (mod 2T) and plane stride = T*T
+// (mod 2T*T) those 32 cells start in 32 different banks, so a warp's loads
+// and atomics at a common stencil offset are conflict-free (2 wavefronts
+// per 8-byte access, the minimum).
+static inline void padded_strides(int e, int T, int &sy, int &sz) {
+    sy = e;
+    while (sy % (2 * T) != T) ++sy;
+    sz = e * sy;
+    while (sz % (2 * T * T) != (T * T) % (2 * T * T)) ++sz;
+}
 
 template <int P>
 __host__ __device__ constexpr int gather_extent(int T) { return T + 2 * (P / 2) + 1; }
@@ -317,14 +332,18 @@ struct TileArgs {
     const real *field[6];
     real scale[4];          // jx, jy, jz, rho
     double inv_scale[4];
+    int *strag[2];          // indices of particles left for the global kernel
+    unsigned long long *nstrag;
 };
 
-#ifndef PIC_TILE_MIN_BLOCKS
-#define PIC_TILE_MIN_BLOCKS 1
-#endif
+// CTAs per SM the register allocation must allow: two for FP32 (measured
+// 1.46x faster at 4th order than one CTA with more registers), one for FP64
+// (which spills under the tighter budget)
+template <typename real>
+constexpr int tile_min_blocks() { return sizeof(real) == 4 ? 2 : 1; }
 
 template <typename real, int P, bool SPIN>
-__global__ void __launch_bounds__(256, PIC_TILE_MIN_BLOCKS) tile_push_kernel(TileArgs<real> ta) {
+__global__ void __launch_bounds__(256, tile_min_blocks<real>()) tile_push_kernel(TileArgs<real> ta) {
     constexpr int H = P / 2;
     constexpr int NL = limbs<real>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -332,8 +351,9 @@ __global__ void __launch_bounds__(256, PIC_TILE_MIN_BLOCKS) tile_push_kernel(Til
     const Geom &g = ta.sp[0].g;
     const int T = ta.t.T;
     const int GE = gather_extent<P>(T), DE = deposit_extent<P>(T);
+    const int gsy = ta.t.gsy, gsz = ta.t.gsz, GS = ta.t.gsize, dsy = ta.t.dsy, dsz = ta.t.dsz, DS = ta.t.dsize;
     const int G2 = GE * GE, G3 = G2 * GE, D2 = DE * DE, D3 = D2 * DE;
-    unsigned *sa = reinterpret_cast<unsigned *>(sf + 6 * G3);   // [component][limb][D3]
+    unsigned *sa = reinterpret_cast<unsigned *>(sf + 6 * GS);   // [component][limb][DS]
     const int nacc = ta.t.nacc;
     const int tile = blockIdx.x;
     const int tx = tile % ta.t.nt[0], ty = (tile / ta.t.nt[0]) % ta.t.nt[1], tz = tile / (ta.t.nt[0] * ta.t.nt[1]);
@@ -369,16 +389,22 @@ __global__ void __launch_bounds__(256, PIC_TILE_MIN_BLOCKS) tile_push_kernel(Til
             real v = 0;
             if (x >= 0 && x < g.f[0] && y >= 0 && y < g.f[1] && z >= 0 && z < g.f[2])
                 v = __ldg(ta.field[c] + g.fi(z, y, x));
-            sf[e] = v;
+            sf[c * GS + lz * gsz + ly * gsy + lx] = v;
         }
-        for (int e = threadIdx.x; e < nacc * NL * D3; e += blockDim.x) sa[e] = 0u;
+        for (int e = threadIdx.x; e < nacc * NL * DS; e += blockDim.x) sa[e] = 0u;
     }
     __syncthreads();
 
     View<const real> fs[6];
 #pragma unroll
-    for (int c = 0; c < 6; ++c) fs[c] = View<const real>{sf + c * G3, GE, G2, -(gO[2] * G2 + gO[1] * GE + gO[0])};
+    for (int c = 0; c < 6; ++c) fs[c] = View<const real>{sf + c * GS, gsy, gsz, -(gO[2] * gsz + gO[1] * gsy + gO[0])};
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    // lanes take 32 consecutive chunks of the cell-sorted list (about one
+    // cell each); with more than 32 cells per tile the warps split over
+    // npass groups of 32 chunks
+    const int ncell_t = T * T * T;
+    const int npass = ncell_t > 32 ? (ncell_t / 32 < nwarp ? ncell_t / 32 : nwarp) : 1;
+    const int pass = warp % npass, r0 = warp / npass, rstep = nwarp / npass;
     const int lo_id[3] = {t0[0] + g.mem - 1, t0[1] + g.mem - 1, t0[2] + g.mem - 1};
 
     // 3. particles of both species
@@ -387,23 +413,20 @@ __global__ void __launch_bounds__(256, PIC_TILE_MIN_BLOCKS) tile_push_kernel(Til
         if (pb[k] <= pa[k]) continue;
         const PushArgs<real> &a = ta.sp[k];
         const long long m = pb[k] - pa[k];
-        const long long chunk = (m + 31) / 32;
-        View<const real> fg[6];
-        GlobalAcc<real> ag;
-        global_views(a, fg, ag);
+        const long long chunk = (m + 32 * npass - 1) / (32 * npass);
         FixedAcc<real, NL> af;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) af.p[c] = sa + c * NL * D3;
-        af.p[3] = (a.rho && nacc == 5) ? sa + (3 + k) * NL * D3 : nullptr;
-        af.lstride = D3;
-        af.sy = DE;
-        af.sz = D2;
-        af.o = -(dO[2] * D2 + dO[1] * DE + dO[0]);
+        for (int c = 0; c < 3; ++c) af.p[c] = sa + c * NL * DS;
+        af.p[3] = (a.rho && nacc == 5) ? sa + (3 + k) * NL * DS : nullptr;
+        af.lstride = DS;
+        af.sy = dsy;
+        af.sz = dsz;
+        af.o = -(dO[2] * dsz + dO[1] * dsy + dO[0]);
 #pragma unroll
         for (int c = 0; c < 4; ++c) af.scale[c] = ta.scale[c];
 #pragma unroll 1
-        for (long long r = warp; r < chunk; r += nwarp) {
-            const long long idx = lane * chunk + r;
+        for (long long r = r0; r < chunk; r += rstep) {
+            const long long idx = (long long)(pass * 32 + lane) * chunk + r;
             if (idx >= m) continue;
             const long long p = pa[k] + idx;
             OldPos<real> o;
@@ -416,7 +439,8 @@ __global__ void __launch_bounds__(256, PIC_TILE_MIN_BLOCKS) tile_push_kernel(Til
             } else if (inside) {
                 push_body<real, P, SPIN, false>(a, p, o, fs, af);
             } else {
-                push_body<real, P, SPIN, true>(a, p, o, fg, ag);
+                // left its tile since the last sort: pushed by the global kernel after this one
+                ta.strag[k][atomicAdd(ta.nstrag + k, 1ull)] = (int)p;
             }
         }
     }
@@ -425,12 +449,12 @@ __global__ void __launch_bounds__(256, PIC_TILE_MIN_BLOCKS) tile_push_kernel(Til
     // 4. reassemble the limbs and flush with one pass of global atomics
     for (int e = threadIdx.x; e < nacc * D3; e += blockDim.x) {
         int c = e / D3, l = e - c * D3;
-        const unsigned *q = sa + c * NL * D3 + l;
-        long long tot;
-        if constexpr (NL == 2) tot = ((long long)(int)q[D3] << 20) + (long long)q[0];
-        else tot = ((long long)(int)q[2 * D3] << 40) + ((long long)q[D3] << 20) + (long long)q[0];
-        if (tot == 0) continue;
         int lz = l / D2, r = l - lz * D2, ly = r / DE, lx = r - ly * DE;
+        const unsigned *q = sa + c * NL * DS + lz * dsz + ly * dsy + lx;
+        long long tot;
+        if constexpr (NL == 2) tot = ((long long)(int)q[DS] << 20) + (long long)(int)q[0];
+        else tot = ((long long)(int)q[2 * DS] << 40) + ((long long)q[DS] << 20) + (long long)q[0];
+        if (tot == 0) continue;
         int x = dO[0] + lx, y = dO[1] + ly, z = dO[2] + lz;
         const real v = (real)((double)tot * ta.inv_scale[c < 3 ? c : 3]);
         if (x >= -1 && x <= g.f[0] && y >= -1 && y <= g.f[1] && z >= -1 && z <= g.f[2])
@@ -440,12 +464,23 @@ __global__ void __launch_bounds__(256, PIC_TILE_MIN_BLOCKS) tile_push_kernel(Til
     }
 }
 
-size_t tile_smem_bytes(const pic_ctx *c) {
+static TileGeom tile_layout(const pic_ctx *c) {
+    TileGeom t = tile_geom(c);
     const int P = c->order == 2 ? 3 : 5;
-    const int T = c->tile;
-    const size_t GE = T + 2 * (P / 2) + 1, DE = T + 2 * (P / 2) + 3;
+    t.GE = t.T + 2 * (P / 2) + 1;
+    t.DE = t.T + 2 * (P / 2) + 3;
+    padded_strides(t.GE, t.T, t.gsy, t.gsz);
+    padded_strides(t.DE, t.T, t.dsy, t.dsz);
+    t.gsize = t.GE * t.gsz;
+    t.dsize = t.DE * t.dsz;
+    t.nacc = c->p.deposit_rho ? 5 : 3;
+    return t;
+}
+
+size_t tile_smem_bytes(const pic_ctx *c) {
+    const TileGeom t = tile_layout(c);
     const size_t rs = c->fp32 ? 4 : 8, nl = c->fp32 ? 2 : 3;
-    return 6 * GE * GE * GE * rs + 5 * nl * DE * DE * DE * 4;
+    return 6 * (size_t)t.gsize * rs + 5 * nl * (size_t)t.dsize * 4;
 }
 
 template <typename real, int P, bool SPIN>
@@ -458,10 +493,7 @@ static void tile_push_t(pic_ctx *c, int mask) {
         ta.active[k] = ((mask >> k) & 1) && c->sp[k].n_host > 0;
         if (ta.active[k]) qw_max = std::max(qw_max, std::fabs(c->p.charge[k]) * c->sp[k].max_abs_w);
     }
-    ta.t = tile_geom(c);
-    ta.t.GE = gather_extent<P>(c->tile);
-    ta.t.DE = deposit_extent<P>(c->tile);
-    ta.t.nacc = c->p.deposit_rho ? 5 : 3;
+    ta.t = tile_layout(c);
     for (int k = 0; k < 5; ++k) ta.ring[k] = (real *)c->ring[k];
     for (int k = 0; k < 6; ++k) ta.field[k] = (const real *)c->field[k];
     // one contribution is at most |q w| d/dt (J: the running sum of ds and the
@@ -475,6 +507,9 @@ static void tile_push_t(pic_ctx *c, int mask) {
         ta.scale[k] = (real)s;
         ta.inv_scale[k] = 1.0 / (double)ta.scale[k];
     }
+    for (int k = 0; k < 2; ++k) ta.strag[k] = c->sp[k].strag;
+    ta.nstrag = c->d_nstrag;
+    cudaMemsetAsync(c->d_nstrag, 0, 2 * sizeof(unsigned long long), c->stream);
     size_t smem = tile_smem_bytes(c);
     cudaFuncSetAttribute(tile_push_kernel<real, P, SPIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int ntiles = c->ntile[0] * c->ntile[1] * c->ntile[2];
@@ -496,6 +531,10 @@ void launch_tile_push(pic_ctx *c, int mask) {
         if (c->order == 2) spin ? tile_push_t<double, 3, true>(c, mask) : tile_push_t<double, 3, false>(c, mask);
         else spin ? tile_push_t<double, 5, true>(c, mask) : tile_push_t<double, 5, false>(c, mask);
     }
+    prof_end(c);
+    prof_begin(c, "straggler_push");
+    for (int k = 0; k < 2; ++k)
+        if (((mask >> k) & 1) && c->sp[k].n_host > 0) launch_push_list(c, k, c->sp[k].strag, c->d_nstrag + k);
     prof_end(c);
     for (int k = 0; k < 2; ++k) {
         Species &s = c->sp[k];
