@@ -50,12 +50,25 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def measured_traffic(precision):
+    """DRAM bytes per particle of the tiled kernel from a committed ncu
+    capture (profiles/tile_push_traffic.json); the traffic grows in
+    proportion to the particles a launch processes."""
+    p = os.path.join(REPO, "profiles", "tile_push_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        return json.load(f)["dram_bytes_per_particle"].get(precision)
+
+
 def workload(name, precision):
     from pic3d_b200 import workloads as W
     if name == "laser_underdense":
         return W.laser_underdense(precision=precision)
     if name == "laser_underdense_small":
         return W.laser_underdense(nx=64, ny=32, nz=32, precision=precision)
+    if name == "laser_underdense_medium":
+        return W.laser_underdense(nx=128, ny=64, nz=64, precision=precision)
     if name == "thermal_scaleup":
         return W.thermal_scaleup(precision=precision)
     raise SystemExit(f"unknown workload {name}")
@@ -315,8 +328,12 @@ def main():
         per_launch = npart / 2.0 if top[0] == "push_gather_deposit" else float(npart)
         bytes_per_launch = per_particle * per_launch
         achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
+        tpp = measured_traffic(prec) if top[0] == "tile_push_gather_deposit" else None
         roof = {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": tpp * per_launch if tpp else None,
+                "traffic_note": "dram read+write bytes per launch, scaled by particles from an ncu capture of "
+                                "128x64x64 cells" if tpp else None,
                 "bytes_per_particle": per_particle, "avg_launch_ms": avg_ms,
                 "share_of_step": top[1][0] / ms}
     kernels = {k: {"ms_total": v[0], "launches": v[1]} for k, v in kern.items()}
