@@ -305,16 +305,8 @@ def main():
     clocks.start()
     ms, kern = timed_steps(sim, args.steps, prof=True)
     clk = clocks.stop()
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        tot = torch.tensor([float(npart)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tot)
-        npart_all = float(tot.item())
-    else:
-        npart_all = float(npart)
-    value = npart_all * args.steps / (ms / 1e3)
+    from pic3d_b200.replicas import combine
+    ms, npart_all, value = combine(ms, npart, args.steps, dist, device="cuda")
 
     # dominant kernel roofline
     peak, peak_kind = measured_peaks()
