@@ -71,6 +71,8 @@ typedef struct PicParams {
     int32_t laser_profile;     /* extension: 0 Gaussian beam (boundary.cpp:38), 1 cubic-B-spline amplitude grid */
     int32_t tile;              /* edge of the shared-memory particle tile in cells (0: default 4, <0: no tiling) */
     int32_t sort_interval;     /* pushes between counting sorts of the particles by cell (0: default 4) */
+    int32_t adjoint;           /* 1: adjoint-capable context (stable particle order, removal marks particles dead;
+                                  absorbing faces only); see pic_adjoint_* */
 } PicParams;
 
 typedef struct pic_ctx pic_ctx;
@@ -167,6 +169,32 @@ int pic_diagnostics(pic_ctx *ctx, double *out, int n);
 int pic_field_diagnostics_noalloc(const PicParams *p, const double *ex, const double *ey, const double *ez,
                                   const double *bx, const double *by, const double *bz, const double *rho0,
                                   const double *rho1, double *out, void *stream);
+
+/* ---- adjoint (no counterpart in the reference) ------------------------
+ * Gradients of a final-state objective with respect to the particle weights
+ * (hence a density profile) and the laser amplitude coefficients
+ * (laser_profile = 1), by a hand-written adjoint of the per-step loop.
+ * Needs a context created with PicParams.adjoint = 1 (absorbing faces,
+ * stable particle order).  Usage, segment by segment from the last:
+ *   pic_checkpoint_save/restore   device copies of the whole state
+ *   pic_adjoint_tape(n) + pic_adjoint_record(1), then pic_initial_push /
+ *   pic_run_steps re-run a segment recording each push's inputs
+ *   pic_adjoint_seed_kinetic      objective = sum w m (gamma-1) of one
+ *                                 species' particles with x in [xlo, xhi)
+ *                                 at the current state; zeroes all adjoints
+ *   pic_adjoint_backward(n)       n recorded steps in reverse
+ *   pic_adjoint_weight_grad       d objective / d weight, per particle in
+ *                                 upload order
+ *   pic_adjoint_profile_grad      d objective / d laser coefficient */
+int pic_checkpoint_save(pic_ctx *ctx, int slot);
+int pic_checkpoint_restore(pic_ctx *ctx, int slot);
+int pic_adjoint_tape(pic_ctx *ctx, int nsteps);
+int pic_adjoint_record(pic_ctx *ctx, int on);
+int pic_adjoint_seed_kinetic(pic_ctx *ctx, int kind, double xlo, double xhi, double *objective);
+int pic_adjoint_backward(pic_ctx *ctx, int nsteps);
+int pic_adjoint_weight_grad(pic_ctx *ctx, int kind, double *grad, int64_t n);
+int pic_adjoint_profile_grad(pic_ctx *ctx, double *grad, int n);
+int pic_adjoint_release(pic_ctx *ctx);
 
 /* ---- per-kernel timing with CUDA events (off by default) ------------- */
 int pic_profile_enable(pic_ctx *ctx, int on);

@@ -33,7 +33,7 @@ class PicParams(ctypes.Structure):
         ("charge", _D * 2), ("mass", _D * 2),
         ("capacity", _I64 * 2),
         ("precision", _I32), ("spin", _I32), ("deposit_rho", _I32),
-        ("laser_envelope", _I32), ("laser_profile", _I32), ("tile", _I32), ("sort_interval", _I32),
+        ("laser_envelope", _I32), ("laser_profile", _I32), ("tile", _I32), ("sort_interval", _I32), ("adjoint", _I32),
     ]
 
 
@@ -52,7 +52,9 @@ EXPORTS = [
     "pic_update_fields_second", "pic_clear_currents", "pic_update_particles", "pic_exchange_particles",
     "pic_exchange_currents", "pic_initial_push", "pic_run_steps", "pic_get_step", "pic_set_step",
     "pic_synchronize", "pic_get_stream", "pic_diagnostics", "pic_profile_enable", "pic_profile_read",
-    "pic_profile_reset", "pic_save", "pic_load", "pic_field_diagnostics_noalloc",
+    "pic_profile_reset", "pic_save", "pic_load", "pic_field_diagnostics_noalloc", "pic_checkpoint_save",
+    "pic_checkpoint_restore", "pic_adjoint_tape", "pic_adjoint_record", "pic_adjoint_seed_kinetic",
+    "pic_adjoint_backward", "pic_adjoint_weight_grad", "pic_adjoint_profile_grad", "pic_adjoint_release",
 ]
 
 
@@ -93,6 +95,15 @@ def load(path: str = LIB_PATH):
     lib.pic_profile_enable.argtypes = [V, ctypes.c_int]
     lib.pic_profile_read.argtypes = [V, P(ctypes.c_char_p), P(_D), P(_I64), ctypes.c_int, P(ctypes.c_int)]
     lib.pic_field_diagnostics_noalloc.argtypes = [P(PicParams)] + [V] * 10
+    lib.pic_checkpoint_save.argtypes = [V, ctypes.c_int]
+    lib.pic_checkpoint_restore.argtypes = [V, ctypes.c_int]
+    lib.pic_adjoint_tape.argtypes = [V, ctypes.c_int]
+    lib.pic_adjoint_record.argtypes = [V, ctypes.c_int]
+    lib.pic_adjoint_seed_kinetic.argtypes = [V, ctypes.c_int, _D, _D, P(_D)]
+    lib.pic_adjoint_backward.argtypes = [V, ctypes.c_int]
+    lib.pic_adjoint_weight_grad.argtypes = [V, ctypes.c_int, V, _I64]
+    lib.pic_adjoint_profile_grad.argtypes = [V, V, ctypes.c_int]
+    lib.pic_adjoint_release.argtypes = [V]
     lib.pic_save.argtypes = [V, ctypes.c_char_p]
     lib.pic_load.argtypes = [V, ctypes.c_char_p]
     _lib = lib

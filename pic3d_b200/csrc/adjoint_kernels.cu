@@ -1,0 +1,1097 @@
+// Hand-written adjoint of the per-timestep loop (no counterpart in the
+// reference), for gradients of a final-state objective with respect to the
+// particle weights (hence a density profile) and the laser's transverse
+// amplitude coefficients.
+//
+// Forward step n (absorbing faces):  BC(t_n) -> E half -> B half -> clear J ->
+// push+deposit -> removal -> B half -> E half.  The adjoint runs the
+// transposes in reverse order.  The field updates are linear, so their
+// transposes need no stored values; the push needs the particles before the
+// push and the fields it gathered (after the first half-update), which a
+// tape records while a checkpointed segment is recomputed.
+//
+//   * Yee transposes: one thread per buffer point in gather form (each
+//     thread writes only its own point, no atomics).
+//   * BC transpose: one thread per face row; adds into neighbours with
+//     atomics and accumulates d objective / d(profile coefficient).
+//   * push adjoint: one thread per particle; recomputes the gather with
+//     shape-derivative weights, takes the Boris Jacobian by forward-mode
+//     dual numbers (three passes of three tangents), contracts the current
+//     adjoint with the Esirkepov factors to get the derivatives of the
+//     deposit with respect to the old and new positions and the weight,
+//     and scatters the gathered-field adjoints back to the grid.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "pic_kernels.cuh"
+#include "push_core.cuh"
+
+namespace pic {
+
+// ---------------------------------------------------------------------------
+// forward-mode dual numbers with N tangents
+
+template <typename T, int N>
+struct Dual {
+    T v;
+    T d[N];
+};
+
+template <typename T, int N>
+__device__ __forceinline__ Dual<T, N> dconst(T v) {
+    Dual<T, N> r;
+    r.v = v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = T(0);
+    return r;
+}
+template <typename T, int N>
+__device__ __forceinline__ Dual<T, N> operator+(const Dual<T, N> &a, const Dual<T, N> &b) {
+    Dual<T, N> r;
+    r.v = a.v + b.v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] + b.d[i];
+    return r;
+}
+template <typename T, int N>
+__device__ __forceinline__ Dual<T, N> operator-(const Dual<T, N> &a, const Dual<T, N> &b) {
+    Dual<T, N> r;
+    r.v = a.v - b.v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] - b.d[i];
+    return r;
+}
+template <typename T, int N>
+__device__ __forceinline__ Dual<T, N> operator*(const Dual<T, N> &a, const Dual<T, N> &b) {
+    Dual<T, N> r;
+    r.v = a.v * b.v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i];
+    return r;
+}
+template <typename T, int N>
+__device__ __forceinline__ Dual<T, N> operator*(const Dual<T, N> &a, T s) {
+    Dual<T, N> r;
+    r.v = a.v * s;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * s;
+    return r;
+}
+template <typename T, int N>
+__device__ __forceinline__ Dual<T, N> operator/(const Dual<T, N> &a, const Dual<T, N> &b) {
+    Dual<T, N> r;
+    T inv = T(1) / b.v;
+    r.v = a.v * inv;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) * inv;
+    return r;
+}
+template <typename T, int N>
+__device__ __forceinline__ Dual<T, N> dsqrt(const Dual<T, N> &a) {
+    Dual<T, N> r;
+    r.v = sqrt(a.v);
+    T h = T(0.5) / r.v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * h;
+    return r;
+}
+
+// Boris rotation and move (particle.cpp:271-315) on duals; inputs p, e, b
+// (fields unscaled), outputs p' and the displacement in cells
+template <typename T, int N>
+__device__ __forceinline__ void boris_dual(const Dual<T, N> (&p)[3], const Dual<T, N> (&e)[3],
+                                           const Dual<T, N> (&b)[3], T qm, const T (&dtd)[3], Dual<T, N> (&pn)[3],
+                                           Dual<T, N> (&disp)[3]) {
+    Dual<T, N> ep[3], bp[3], p1[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        ep[d] = e[d] * qm;
+        bp[d] = b[d] * qm;
+        p1[d] = p[d] + ep[d];
+    }
+    Dual<T, N> one = dconst<T, N>(T(1));
+    Dual<T, N> gm1 = dsqrt(one + (p1[0] * p1[0] + p1[1] * p1[1] + p1[2] * p1[2]));
+    Dual<T, N> t[3] = {bp[0] / gm1, bp[1] / gm1, bp[2] / gm1};
+    Dual<T, N> tt = dconst<T, N>(T(2)) / (one + t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+    Dual<T, N> s[3] = {t[0] * tt, t[1] * tt, t[2] * tt};
+    Dual<T, N> p2[3] = {p1[0] + (p1[1] * t[2] - p1[2] * t[1]), p1[1] + (p1[2] * t[0] - p1[0] * t[2]),
+                        p1[2] + (p1[0] * t[1] - p1[1] * t[0])};
+    pn[0] = p1[0] + (p2[1] * s[2] - p2[2] * s[1]) + ep[0];
+    pn[1] = p1[1] + (p2[2] * s[0] - p2[0] * s[2]) + ep[1];
+    pn[2] = p1[2] + (p2[0] * s[1] - p2[1] * s[0]) + ep[2];
+    Dual<T, N> gam = dsqrt(one + (pn[0] * pn[0] + pn[1] * pn[1] + pn[2] * pn[2]));
+#pragma unroll
+    for (int d = 0; d < 3; ++d) disp[d] = (pn[d] / gam) * dtd[d];
+}
+
+// derivatives of the shape weights with respect to the position
+template <typename real>
+__device__ __forceinline__ void shape_derivs(real d, real (&w)[3]) {
+    const real h = real(0.5);
+    w[0] = -(h - d);
+    w[1] = real(-2) * d;
+    w[2] = h + d;
+}
+template <typename real>
+__device__ __forceinline__ void shape_derivs(real d, real (&w)[5]) {
+    real u, u2;
+    u = d - real(0.5);
+    u2 = u * u;
+    w[0] = u2 * u * real(1.0 / 6.0);
+    u = d + real(1.0);
+    u2 = u * u;
+    w[1] = -u2 * u * real(4.0 / 6.0) + u2 * real(15.0 / 6.0) - u * real(10.0 / 4.0) + real(5.0 / 24.0);
+    u = d;
+    u2 = u * u;
+    w[2] = u2 * u - u * real(5.0 / 4.0);
+    u = d - real(1.0);
+    u2 = u * u;
+    w[3] = -u2 * u * real(4.0 / 6.0) - u2 * real(15.0 / 6.0) - u * real(10.0 / 4.0) - real(5.0 / 24.0);
+    u = d + real(0.5);
+    u2 = u * u;
+    w[4] = u2 * u * real(1.0 / 6.0);
+}
+
+// gather of one component with its gradient with respect to the position
+template <typename real, int P>
+__device__ __forceinline__ void gather_grad(const real *f, const Geom &g, int i0, int j0, int k0,
+                                            const real (&wx)[P], const real (&wy)[P], const real (&wz)[P],
+                                            const real (&dx)[P], const real (&dy)[P], const real (&dz)[P], real &e,
+                                            real (&gr)[3]) {
+    e = 0;
+    gr[0] = gr[1] = gr[2] = 0;
+    for (int k = 0; k < P; ++k) {
+        real a = 0, ax = 0, ay = 0;
+#pragma unroll
+        for (int j = 0; j < P; ++j) {
+            const real *row = f + g.fi(k0 + k, j0 + j, i0);
+            real s = 0, sd = 0;
+#pragma unroll
+            for (int i = 0; i < P; ++i) {
+                real v = __ldg(row + i);
+                s += wx[i] * v;
+                sd += dx[i] * v;
+            }
+            a += wy[j] * s;
+            ax += wy[j] * sd;
+            ay += dy[j] * s;
+        }
+        const real wzk = pick(wz, k), dzk = pick(dz, k);
+        e += wzk * a;
+        gr[0] += wzk * ax;
+        gr[1] += wzk * ay;
+        gr[2] += dzk * a;
+    }
+}
+
+template <typename real, int P>
+__device__ __forceinline__ void scatter_adj(real *f, const Geom &g, int i0, int j0, int k0, const real (&wx)[P],
+                                            const real (&wy)[P], const real (&wz)[P], real lam) {
+    if (lam == real(0)) return;
+    for (int k = 0; k < P; ++k) {
+        const real lk = lam * pick(wz, k);
+#pragma unroll
+        for (int j = 0; j < P; ++j) {
+            real *row = f + g.fi(k0 + k, j0 + j, i0);
+            const real lj = lk * wy[j];
+#pragma unroll
+            for (int i = 0; i < P; ++i) atomic_add(row + i, lj * wx[i]);
+        }
+    }
+}
+
+// union-span arrays of a quantity of the old (a0 at centre i1) and new (a1
+// at centre i2) positions, as span1d does for the weights
+template <typename T, int P>
+__device__ __forceinline__ void span_pair(int i1, const T (&a0)[P], int i2, const T (&a1)[P], T (&u0)[P + 1],
+                                          T (&u1)[P + 1]) {
+    const int lo = min(i1, i2);
+    const bool o0 = i1 != lo, o1 = i2 != lo;
+#pragma unroll
+    for (int a = 0; a <= P; ++a) {
+        u0[a] = o0 ? (a >= 1 ? a0[a - 1] : T(0)) : (a < P ? a0[a] : T(0));
+        u1[a] = o1 ? (a >= 1 ? a1[a - 1] : T(0)) : (a < P ? a1[a] : T(0));
+    }
+}
+
+// Adjoint of one Esirkepov component.  Axis `c` carries the running sum of
+// ds = s1 - s0, axes `u` and `v` the weight
+// W = 1/3 s0u s0v + 1/6 s1u s0v + 1/6 s0u s1v + 1/3 s1u s1v.
+// Returns G1 = sum(lam * J) / w and adds dG1/ds0, dG1/ds1 into g0, g1.
+template <int P>
+__device__ __forceinline__ double esirkepov_adj(const double *lam, int sc, int su, int sv, int lc, int lu, int lv,
+                                                double coef, const double (&s0c)[P + 1], const double (&s1c)[P + 1],
+                                                const double (&s0u)[P + 1], const double (&s1u)[P + 1],
+                                                const double (&s0v)[P + 1], const double (&s1v)[P + 1],
+                                                double (&g0c)[P + 1], double (&g1c)[P + 1], double (&g0u)[P + 1],
+                                                double (&g1u)[P + 1], double (&g0v)[P + 1], double (&g1v)[P + 1]) {
+    constexpr double third = 1.0 / 3.0, sixth = 1.0 / 6.0;
+    double C[P + 1];
+    double acc = 0.0;
+#pragma unroll
+    for (int a = 0; a <= P; ++a) {
+        acc += s1c[a] - s0c[a];
+        C[a] = (a < lc - 1) ? acc : 0.0;   // the last running-sum point is not deposited
+    }
+    double M[P + 1];
+#pragma unroll
+    for (int a = 0; a <= P; ++a) M[a] = 0.0;
+    double G = 0.0;
+    for (int b = 0; b < lv; ++b) {
+        const double s0b = pick(s0v, b), s1b = pick(s1v, b);
+        double dv0 = 0.0, dv1 = 0.0;
+#pragma unroll
+        for (int a = 0; a <= P; ++a) {
+            if (a >= lu) break;
+            const double W = third * s0u[a] * s0b + sixth * s1u[a] * s0b + sixth * s0u[a] * s1b + third * s1u[a] * s1b;
+            double T = 0.0;
+            const double *row = lam + b * sv + a * su;
+#pragma unroll
+            for (int q = 0; q < P; ++q) {
+                if (q >= lc - 1) break;
+                const double l = row[q * sc];
+                T += C[q] * l;
+                M[q] += l * W;
+            }
+            G += T * W;
+            g0u[a] += coef * T * (third * s0b + sixth * s1b);
+            g1u[a] += coef * T * (sixth * s0b + third * s1b);
+            dv0 += T * (third * s0u[a] + sixth * s1u[a]);
+            dv1 += T * (sixth * s0u[a] + third * s1u[a]);
+        }
+        // add into g0v[b], g1v[b] for a run-time b
+#pragma unroll
+        for (int q = 0; q <= P; ++q)
+            if (q == b) {
+                g0v[q] += coef * dv0;
+                g1v[q] += coef * dv1;
+            }
+    }
+    // dG/dds(q') = coef * sum_{q >= q'} M(q); ds = s1 - s0
+    double suf = 0.0;
+#pragma unroll
+    for (int q = P; q >= 0; --q) {
+        suf += M[q];
+        g1c[q] += coef * suf;
+        g0c[q] -= coef * suf;
+    }
+    return coef * G;
+}
+
+template <typename real>
+struct AdjPushArgs {
+    Geom g;
+    CellPack cp;
+    long long n;
+    // tape: particles before the push, fields after the first half-update
+    const double *x, *y, *z;
+    const int *cell;
+    const float *ox, *oy, *oz;
+    const real *px, *py, *pz;
+    const unsigned char *dead;
+    const real *f[6];
+    const real *w;
+    // adjoints
+    const real *lj[3];         // d objective / dJ (ring buffers)
+    real *lf[6];               // d objective / d(E, B) after the first half-update (field buffers)
+    real *lx, *ly, *lz, *lpx, *lpy, *lpz;   // per particle, in: after the push, out: before it
+    double *lw;                // per particle, accumulated
+    real qm, charge;
+    real dt_d[3];
+    double d_dt[3];
+    int scatter_fields;        // 0 for the t = 0 push (fields identically zero there)
+    unsigned *status;
+};
+
+template <typename real, int P>
+__global__ void __launch_bounds__(128) adj_push_kernel(AdjPushArgs<real> a) {
+    constexpr bool F64 = sizeof(real) == 8;
+    constexpr int H = P / 2;
+    const Geom &g = a.g;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n;
+         p += (long long)gridDim.x * blockDim.x) {
+        if (a.dead && a.dead[p]) continue;
+        // ---- old position --------------------------------------------------
+        int ip[3], id[3], cc[3] = {0, 0, 0};
+        real dp[3], dd[3];
+        double xd[3] = {0, 0, 0};
+        real oo[3] = {0, 0, 0};
+        if constexpr (F64) {
+            xd[0] = a.x[p];
+            xd[1] = a.y[p];
+            xd[2] = a.z[p];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                double xc = xd[d] - (double)(1 - g.mem);
+                ip[d] = (int)(xc + 0.5);
+                dp[d] = xc - (double)ip[d];
+                id[d] = (int)xc;
+                dd[d] = (xc - 0.5) - (double)id[d];
+            }
+        } else {
+            a.cp.unpack(a.cell[p], cc[0], cc[1], cc[2]);
+            oo[0] = a.ox[p];
+            oo[1] = a.oy[p];
+            oo[2] = a.oz[p];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                int b = cc[d] + g.mem - 1;
+                bool up = oo[d] >= 0.5f;
+                ip[d] = b + (up ? 1 : 0);
+                dp[d] = up ? oo[d] - 1.0f : oo[d];
+                id[d] = b;
+                dd[d] = oo[d] - 0.5f;
+            }
+        }
+        bool ok = true;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) ok = ok && id[d] >= H && ip[d] <= g.f[d] - 1 - H;
+        if (!ok) {
+            set_status(a.status, ST_OOB);
+            continue;
+        }
+        real wp[3][P], wd[3][P], gp[3][P], gd[3][P];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            shape_weights(dp[d], wp[d]);
+            shape_weights(dd[d], wd[d]);
+            shape_derivs(dp[d], gp[d]);
+            shape_derivs(dd[d], gd[d]);
+        }
+        // ---- gather with gradients (Yee staggering, particle.cpp:207-259) -
+        real ev[6], eg[6][3];
+        gather_grad<real, P>(a.f[0], g, id[0] - H, ip[1] - H, ip[2] - H, wd[0], wp[1], wp[2], gd[0], gp[1], gp[2], ev[0], eg[0]);
+        gather_grad<real, P>(a.f[1], g, ip[0] - H, id[1] - H, ip[2] - H, wp[0], wd[1], wp[2], gp[0], gd[1], gp[2], ev[1], eg[1]);
+        gather_grad<real, P>(a.f[2], g, ip[0] - H, ip[1] - H, id[2] - H, wp[0], wp[1], wd[2], gp[0], gp[1], gd[2], ev[2], eg[2]);
+        gather_grad<real, P>(a.f[3], g, ip[0] - H, id[1] - H, id[2] - H, wp[0], wd[1], wd[2], gp[0], gd[1], gd[2], ev[3], eg[3]);
+        gather_grad<real, P>(a.f[4], g, id[0] - H, ip[1] - H, id[2] - H, wd[0], wp[1], wd[2], gd[0], gp[1], gd[2], ev[4], eg[4]);
+        gather_grad<real, P>(a.f[5], g, id[0] - H, id[1] - H, ip[2] - H, wd[0], wd[1], wp[2], gd[0], gd[1], gp[2], ev[5], eg[5]);
+        // ---- Boris Jacobian: three passes of three tangents (p, e, b) -----
+        const real pin[3] = {a.px[p], a.py[p], a.pz[p]};
+        real jac[6][9];   // d(p', disp) / d(p, e, b)
+        real pn_v[3], disp_v[3];
+#pragma unroll
+        for (int pass = 0; pass < 3; ++pass) {
+            Dual<real, 3> P_[3], E_[3], B_[3], pn[3], ds[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                P_[d] = dconst<real, 3>(pin[d]);
+                E_[d] = dconst<real, 3>(ev[d]);
+                B_[d] = dconst<real, 3>(ev[3 + d]);
+            }
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                if (pass == 0) P_[d].d[d] = real(1);
+                if (pass == 1) E_[d].d[d] = real(1);
+                if (pass == 2) B_[d].d[d] = real(1);
+            }
+            boris_dual<real, 3>(P_, E_, B_, a.qm, a.dt_d, pn, ds);
+#pragma unroll
+            for (int o = 0; o < 3; ++o) {
+#pragma unroll
+                for (int t = 0; t < 3; ++t) {
+                    jac[o][3 * pass + t] = pn[o].d[t];
+                    jac[3 + o][3 * pass + t] = ds[o].d[t];
+                }
+                pn_v[o] = pn[o].v;
+                disp_v[o] = ds[o].v;
+            }
+        }
+        // ---- new position, as the forward deposit forms it ----------------
+        int i2[3];
+        double d2[3], d0[3];
+        if constexpr (F64) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                double xc = (xd[d] + (double)disp_v[d]) - (double)(1 - g.mem);
+                i2[d] = (int)(xc + 0.5);
+                d2[d] = xc - (double)i2[d];
+                d0[d] = dp[d];
+            }
+        } else {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                double u = (double)oo[d] + (double)disp_v[d];
+                double f = floor(u + 0.5);
+                i2[d] = cc[d] + g.mem - 1 + (int)f;
+                d2[d] = u - f;
+                d0[d] = (double)dp[d];
+            }
+        }
+        bool cfl = abs(i2[0] - ip[0]) <= 1 && abs(i2[1] - ip[1]) <= 1 && abs(i2[2] - ip[2]) <= 1;
+        if (!cfl) {
+            set_status(a.status, ST_CFL);
+            continue;
+        }
+        // ---- deposit adjoint ----------------------------------------------
+        double s0[3][P + 1], s1[3][P + 1], t0[3][P + 1], t1[3][P + 1];   // weights and their derivatives
+        double g0[3][P + 1], g1[3][P + 1];                                // dG1 / d(weights)
+        int base[3], len[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double w0[P], w1[P], v0[P], v1[P];
+            shape_weights(d0[d], w0);
+            shape_weights(d2[d], w1);
+            shape_derivs(d0[d], v0);
+            shape_derivs(d2[d], v1);
+            span_pair<double, P>(ip[d], w0, i2[d], w1, s0[d], s1[d]);
+            span_pair<double, P>(ip[d], v0, i2[d], v1, t0[d], t1[d]);
+            base[d] = min(ip[d], i2[d]) - H;
+            len[d] = P + abs(i2[d] - ip[d]);
+#pragma unroll
+            for (int q = 0; q <= P; ++q) g0[d][q] = g1[d][q] = 0.0;
+        }
+        const double qd = (double)a.charge;
+        double G1 = 0.0;
+        double lbuf[(P + 1) * (P + 1) * (P + 1)];
+        // Jx: running sum along x, weight from y and z (particle.cpp:427-450)
+#pragma unroll 1
+        for (int comp = 0; comp < 3; ++comp) {
+            const real *lj = a.lj[comp];
+            for (int k = 0; k < len[2]; ++k)
+                for (int j = 0; j < len[1]; ++j)
+                    for (int i = 0; i < len[0]; ++i)
+                        lbuf[(k * (P + 1) + j) * (P + 1) + i] =
+                            (double)__ldg(lj + g.ri(base[2] + k, base[1] + j, base[0] + i));
+            const int sX = 1, sY = P + 1, sZ = (P + 1) * (P + 1);
+            if (comp == 0)
+                G1 += esirkepov_adj<P>(lbuf, sX, sY, sZ, len[0], len[1], len[2], -qd * a.d_dt[0], s0[0], s1[0],
+                                       s0[1], s1[1], s0[2], s1[2], g0[0], g1[0], g0[1], g1[1], g0[2], g1[2]);
+            else if (comp == 1)
+                G1 += esirkepov_adj<P>(lbuf, sY, sX, sZ, len[1], len[0], len[2], -qd * a.d_dt[1], s0[1], s1[1],
+                                       s0[0], s1[0], s0[2], s1[2], g0[1], g1[1], g0[0], g1[0], g0[2], g1[2]);
+            else
+                G1 += esirkepov_adj<P>(lbuf, sZ, sX, sY, len[2], len[0], len[1], -qd * a.d_dt[2], s0[2], s1[2],
+                                       s0[0], s1[0], s0[1], s1[1], g0[2], g1[2], g0[0], g1[0], g0[1], g1[1]);
+        }
+        const double wgt = (double)a.w[p];
+        a.lw[p] += G1;
+        double dGx0[3], dGx1[3];   // d G / d x_old, d G / d x_new
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double s_0 = 0.0, s_1 = 0.0;
+#pragma unroll
+            for (int q = 0; q <= P; ++q) {
+                s_0 += g0[d][q] * t0[d][q];
+                s_1 += g1[d][q] * t1[d][q];
+            }
+            dGx0[d] = wgt * s_0;
+            dGx1[d] = wgt * s_1;
+        }
+        // ---- chain rule ---------------------------------------------------
+        const real lxn[3] = {a.lx[p] + (real)dGx1[0], a.ly[p] + (real)dGx1[1], a.lz[p] + (real)dGx1[2]};
+        const real lpn[3] = {a.lpx[p], a.lpy[p], a.lpz[p]};
+        real lin[9];
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+            real s = 0;
+#pragma unroll
+            for (int o = 0; o < 3; ++o) s += lpn[o] * jac[o][t] + lxn[o] * jac[3 + o][t];
+            lin[t] = s;
+        }
+        real lxo[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            real s = lxn[d] + (real)dGx0[d];
+#pragma unroll
+            for (int c = 0; c < 6; ++c) s += lin[3 + c] * eg[c][d];
+            lxo[d] = s;
+        }
+        a.lx[p] = lxo[0];
+        a.ly[p] = lxo[1];
+        a.lz[p] = lxo[2];
+        a.lpx[p] = lin[0];
+        a.lpy[p] = lin[1];
+        a.lpz[p] = lin[2];
+        if (a.scatter_fields) {
+            scatter_adj<real, P>(a.lf[0], g, id[0] - H, ip[1] - H, ip[2] - H, wd[0], wp[1], wp[2], lin[3]);
+            scatter_adj<real, P>(a.lf[1], g, ip[0] - H, id[1] - H, ip[2] - H, wp[0], wd[1], wp[2], lin[4]);
+            scatter_adj<real, P>(a.lf[2], g, ip[0] - H, ip[1] - H, id[2] - H, wp[0], wp[1], wd[2], lin[5]);
+            scatter_adj<real, P>(a.lf[3], g, ip[0] - H, id[1] - H, id[2] - H, wp[0], wd[1], wd[2], lin[6]);
+            scatter_adj<real, P>(a.lf[4], g, id[0] - H, ip[1] - H, id[2] - H, wd[0], wp[1], wd[2], lin[7]);
+            scatter_adj<real, P>(a.lf[5], g, id[0] - H, id[1] - H, ip[2] - H, wd[0], wd[1], wp[2], lin[8]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// transposes of the Yee half-updates (physical cells only, absorbing faces)
+
+__device__ __forceinline__ bool physical(const Geom &g, int k, int j, int i) {
+    return i >= g.mem && i < g.n[0] + g.mem && j >= g.mem && j < g.n[1] + g.mem && k >= g.mem && k < g.n[2] + g.mem;
+}
+
+// transpose of E += h (curl B - J): lamB += h curl^T lamE, lamJ -= h lamE
+template <typename real>
+__global__ void adj_update_e_kernel(Geom g, const real *lex, const real *ley, const real *lez, real *lbx, real *lby,
+                                    real *lbz, real *ljx, real *ljy, real *ljz, real h, real idx, real idy, real idz) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.fsz) return;
+    int i = (int)(t % g.f[0]), j = (int)((t / g.f[0]) % g.f[1]), k = (int)(t / g.fxy);
+    const int q = (int)t;
+    auto L = [&](const real *a, int kk, int jj, int ii) -> real {
+        return (ii < g.f[0] && jj < g.f[1] && kk < g.f[2] && physical(g, kk, jj, ii)) ? a[g.fi(kk, jj, ii)] : real(0);
+    };
+    real ex0 = L(lex, k, j, i), ey0 = L(ley, k, j, i), ez0 = L(lez, k, j, i);
+    lbz[q] += h * idy * (ex0 - L(lex, k, j + 1, i)) - h * idx * (ey0 - L(ley, k, j, i + 1));
+    lby[q] += -h * idz * (ex0 - L(lex, k + 1, j, i)) + h * idx * (ez0 - L(lez, k, j, i + 1));
+    lbx[q] += h * idz * (ey0 - L(ley, k + 1, j, i)) - h * idy * (ez0 - L(lez, k, j + 1, i));
+    if (physical(g, k, j, i)) {
+        const int r = g.ri(k, j, i);
+        ljx[r] -= h * ex0;
+        ljy[r] -= h * ey0;
+        ljz[r] -= h * ez0;
+    }
+}
+
+// transpose of B -= h curl E: lamE -= h curl^T lamB
+template <typename real>
+__global__ void adj_update_b_kernel(Geom g, real *lex, real *ley, real *lez, const real *lbx, const real *lby,
+                                    const real *lbz, real h, real idx, real idy, real idz) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.fsz) return;
+    int i = (int)(t % g.f[0]), j = (int)((t / g.f[0]) % g.f[1]), k = (int)(t / g.fxy);
+    const int q = (int)t;
+    auto L = [&](const real *a, int kk, int jj, int ii) -> real {
+        return (ii >= 0 && jj >= 0 && kk >= 0 && physical(g, kk, jj, ii)) ? a[g.fi(kk, jj, ii)] : real(0);
+    };
+    real bx0 = L(lbx, k, j, i), by0 = L(lby, k, j, i), bz0 = L(lbz, k, j, i);
+    lez[q] += -h * idy * L(lbx, k, j - 1, i) + h * idy * bx0 + h * idx * L(lby, k, j, i - 1) - h * idx * by0;
+    ley[q] += h * idz * L(lbx, k - 1, j, i) - h * idz * bx0 - h * idx * L(lbz, k, j, i - 1) + h * idx * bz0;
+    lex[q] += -h * idz * L(lby, k - 1, j, i) + h * idz * by0 + h * idy * L(lbz, k, j - 1, i) - h * idy * bz0;
+}
+
+// transpose of radiating_boundary (boundary.cpp:42-99) at time t: the two
+// B columns it overwrites hand their adjoint to the inputs of the formula
+// and to the laser source; d source / d coefficient accumulates in lprof.
+struct AdjBcArgs {
+    Geom g;
+    double dt, dx, dy, dz;
+    double Pi, omega, l0, amp, dur, start, waist, xfocus, yfocus, zfocus, phase, time;
+    int pol, envelope, profile_n;
+    double *lprof;
+};
+
+__device__ double adj_envelope(const AdjBcArgs &L, double t) {
+    t = t - L.start;
+    if (L.envelope == 1) {
+        if (t < 0.0 || t > 3.0 * L.dur) return 0.0;
+        double r = (t - 1.5 * L.dur) / L.dur;
+        return L.amp * exp(-2.0 * log(2.0) * r * r);
+    }
+    return (t >= 0.0 && t <= L.dur) ? L.amp * sin(L.Pi * t / L.dur) : 0.0;
+}
+
+template <typename real>
+__global__ void adj_bc_kernel(AdjBcArgs A, real *lex, real *ley, real *lez, real *lbx, real *lby, real *lbz,
+                              real *ljy, real *ljz) {
+    (void)lex;
+    const Geom &g = A.g;
+    int iy = blockIdx.x * blockDim.x + threadIdx.x;
+    int iz = blockIdx.y * blockDim.y + threadIdx.y;
+    if (iy >= g.n[1] || iz >= g.n[2]) return;
+    iy += g.mem;
+    iz += g.mem;
+    const double alpha = 1 / (1 + A.dt / A.dx), beta = 1 - A.dt / A.dx;
+    const int m = g.mem, L = g.n[0];
+    double lsrc = 0.0;
+    for (int side = 0; side < 2; ++side) {
+        const int col = side == 0 ? m : L, out = side == 0 ? m - 1 : L + 1;
+        const int c = g.fi(iz, iy, col), o = g.fi(iz, iy, out), rc = g.ri(iz, iy, col);
+        const double Lz = lbz[o], Ly = lby[o];
+        lbz[o] = 0;
+        lby[o] = 0;
+        const double sg = side == 0 ? 1.0 : -1.0;   // right column: signs of the E and J terms flip
+        atomic_add(ley + c, (real)(-2 * alpha * sg * Lz));
+        atomic_add(lbx + c, (real)(-alpha * A.dt / A.dz * Lz + alpha * A.dt / A.dy * Ly));
+        atomic_add(lbx + c - g.fxy, (real)(alpha * A.dt / A.dz * Lz));
+        atomic_add(lbx + c - g.f[0], (real)(-alpha * A.dt / A.dy * Ly));
+        atomic_add(lbz + c, (real)(-alpha * beta * Lz));
+        atomic_add(ljy + rc, (real)(-alpha * A.dt * sg * Lz));
+        atomic_add(lez + c, (real)(2 * alpha * sg * Ly));
+        atomic_add(lby + c, (real)(-alpha * beta * Ly));
+        atomic_add(ljz + rc, (real)(alpha * A.dt * sg * Ly));
+        if (side == 0) {
+            if (A.pol == 1 || A.pol == 3) lsrc += 4 * alpha * Lz;
+            if (A.pol == 2 || A.pol == 3) lsrc += -4 * alpha * Ly;
+        }
+    }
+    if (!A.lprof || lsrc == 0.0) return;
+    // d source / d coefficient (laser_profile = 1): -env * B_c(u) B_b(v) * cos(PHI + phase)
+    const double k = 2.0 * A.Pi / A.l0, rl = 0.5 * k * A.waist * A.waist, xe = 0.0 - A.xfocus;
+    const double y = iy * A.dy - A.yfocus, z = iz * A.dz - A.zfocus;
+    const double q = xe / rl, w = A.waist * sqrt(1 + q * q);
+    const double PHI = (xe / rl) * (y * y + z * z) / w / w - atan(xe / rl) + k * xe - A.omega * A.time;
+    const double f = -1.0 * adj_envelope(A, A.time) * cos(PHI + A.phase);
+    if (f == 0.0) return;
+    const int nc = A.profile_n;
+    const double u = ((double)(iy - g.mem) + 0.5) / (double)g.n[1] * (double)(nc - 1);
+    const double v = ((double)(iz - g.mem) + 0.5) / (double)g.n[2] * (double)(nc - 1);
+    for (int b = 0; b < nc; ++b) {
+        double wv = cubic_bspline(v - b);
+        if (wv == 0.0) continue;
+        for (int cidx = 0; cidx < nc; ++cidx) {
+            double wu = cubic_bspline(u - cidx);
+            if (wu == 0.0) continue;
+            atomicAdd(A.lprof + b * nc + cidx, lsrc * f * wu * wv);
+        }
+    }
+}
+
+// objective: kinetic energy sum w m (gamma - 1) of the alive particles of a
+// species with x in [xlo, xhi); seeds d objective / d p and / d w
+template <typename real>
+__global__ void adj_seed_kinetic_kernel(Geom g, CellPack cp, int fp32, long long n, const double *x, const int *cell,
+                                        const float *ox, const real *px, const real *py, const real *pz,
+                                        const real *w, const unsigned char *dead, double mass, double xlo,
+                                        double xhi, real *lpx, real *lpy, real *lpz, double *lw, double *loss) {
+    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double contrib = 0.0;
+    if (p < n && !(dead && dead[p])) {
+        double xp;
+        if (fp32) {
+            int cx, cy, cz;
+            cp.unpack(cell[p], cx, cy, cz);
+            xp = (double)cx + (double)ox[p];
+        } else {
+            xp = x[p];
+        }
+        if (xp >= xlo && xp < xhi) {
+            double a = px[p], b = py[p], c = pz[p];
+            double u2 = a * a + b * b + c * c, gam = sqrt(1.0 + u2);
+            double gm1 = u2 / (gam + 1.0);
+            double wt = w[p];
+            contrib = wt * mass * gm1;
+            lpx[p] += (real)(wt * mass * a / gam);
+            lpy[p] += (real)(wt * mass * b / gam);
+            lpz[p] += (real)(wt * mass * c / gam);
+            lw[p] += mass * gm1;
+        }
+    }
+    // warp reduction of the loss
+    for (int o = 16; o > 0; o >>= 1) contrib += __shfl_down_sync(0xffffffffu, contrib, o);
+    if ((threadIdx.x & 31) == 0 && contrib != 0.0) atomicAdd(loss, contrib);
+}
+
+}  // namespace pic
+
+// ===========================================================================
+// host side: checkpoints, tape and the C ABI
+// ===========================================================================
+
+using namespace pic;
+
+struct Blob {
+    std::vector<std::pair<void *, size_t>> parts;   // (device pointer, bytes) at save time
+    void *buf = nullptr;
+    size_t bytes = 0;
+    int step = 0;
+    int cur[2] = {0, 0};
+    long long count[2] = {0, 0};
+};
+
+struct AdjState {
+    std::vector<Blob> ckpt;
+    std::vector<Blob> tape;
+    int tape_len = 0;
+    bool recording = false;
+    // adjoint arrays
+    void *lf[6] = {};        // field-buffer adjoints (E, B)
+    void *lj[3] = {};        // ring-buffer adjoints (J)
+    void *lpart[2][6] = {};  // per species: lx, ly, lz, lpx, lpy, lpz
+    double *lw[2] = {};
+    double *lprof = nullptr;
+    double *loss = nullptr;
+    int nprof = 0;
+};
+
+static std::vector<std::pair<pic_ctx *, AdjState *>> g_adj;
+
+static AdjState *adj_of(pic_ctx *c, bool create) {
+    for (auto &e : g_adj)
+        if (e.first == c) return e.second;
+    if (!create) return nullptr;
+    g_adj.push_back({c, new AdjState()});
+    return g_adj.back().second;
+}
+
+static size_t rsize(const pic_ctx *c) { return c->fp32 ? 4 : 8; }
+
+// pieces of the particle state (current positions, momenta, dead flags)
+static void particle_parts(pic_ctx *c, std::vector<std::pair<void *, size_t>> &v) {
+    for (int k = 0; k < 2; ++k) {
+        Species &s = c->sp[k];
+        size_t n = (size_t)s.n_host;
+        if (n == 0) continue;
+        if (c->fp32) {
+            v.push_back({s.a.cell[s.cur], n * 4});
+            v.push_back({s.a.ox[s.cur], n * 4});
+            v.push_back({s.a.oy[s.cur], n * 4});
+            v.push_back({s.a.oz[s.cur], n * 4});
+        } else {
+            v.push_back({s.a.x[s.cur], n * 8});
+            v.push_back({s.a.y[s.cur], n * 8});
+            v.push_back({s.a.z[s.cur], n * 8});
+        }
+        v.push_back({s.a.px, n * rsize(c)});
+        v.push_back({s.a.py, n * rsize(c)});
+        v.push_back({s.a.pz, n * rsize(c)});
+        if (s.dead) v.push_back({s.dead, n});
+    }
+}
+
+static int blob_save(pic_ctx *c, Blob &b, const std::vector<std::pair<void *, size_t>> &parts) {
+    size_t total = 0;
+    for (auto &p : parts) total += (p.second + 255) & ~(size_t)255;
+    if (b.bytes < total) {
+        if (b.buf) cudaFree(b.buf);
+        b.buf = nullptr;
+        b.bytes = 0;
+        if (cudaMalloc(&b.buf, total) != cudaSuccess) {
+            c->err = "adjoint: out of device memory for a checkpoint / tape slot";
+            return PIC_ENOMEM;
+        }
+        b.bytes = total;
+    }
+    b.parts = parts;
+    size_t off = 0;
+    for (auto &p : parts) {
+        cudaMemcpyAsync((char *)b.buf + off, p.first, p.second, cudaMemcpyDeviceToDevice, c->stream);
+        off += (p.second + 255) & ~(size_t)255;
+    }
+    b.step = c->step;
+    for (int k = 0; k < 2; ++k) {
+        b.cur[k] = c->sp[k].cur;
+        b.count[k] = c->sp[k].n_host;
+    }
+    return PIC_OK;
+}
+
+// the tape slot's device pointer of part `idx`
+static void *blob_part(const Blob &b, int idx) {
+    size_t off = 0;
+    for (int i = 0; i < idx; ++i) off += (b.parts[i].second + 255) & ~(size_t)255;
+    return (char *)b.buf + off;
+}
+
+namespace pic {
+// called by the step orchestration right before each push while recording
+void adjoint_record_hook(pic_ctx *c) {
+    AdjState *A = adj_of(c, false);
+    if (!A || !A->recording) return;
+    if (A->tape_len >= (int)A->tape.size()) {
+        c->err = "adjoint tape full";
+        return;
+    }
+    std::vector<std::pair<void *, size_t>> parts;
+    particle_parts(c, parts);
+    for (int f = 0; f < 6; ++f) parts.push_back({c->field[f], (size_t)c->g.fsz * rsize(c)});
+    if (blob_save(c, A->tape[A->tape_len], parts) == PIC_OK) A->tape_len++;
+}
+}  // namespace pic
+
+static int ensure_adj_arrays(pic_ctx *c, AdjState *A) {
+    const size_t rs = rsize(c);
+    auto alloc = [&](void **p, size_t bytes) -> bool {
+        if (*p) return true;
+        if (cudaMalloc(p, bytes) != cudaSuccess) return false;
+        return true;
+    };
+    bool ok = true;
+    for (int f = 0; f < 6; ++f) ok = ok && alloc(&A->lf[f], (size_t)c->g.fsz * rs);
+    for (int f = 0; f < 3; ++f) ok = ok && alloc(&A->lj[f], (size_t)c->g.rsz * rs);
+    for (int k = 0; k < 2; ++k) {
+        size_t n = (size_t)std::max<int64_t>(c->sp[k].cap, 1);
+        for (int q = 0; q < 6; ++q) ok = ok && alloc(&A->lpart[k][q], n * rs);
+        ok = ok && alloc((void **)&A->lw[k], n * sizeof(double));
+    }
+    ok = ok && alloc((void **)&A->loss, sizeof(double));
+    int np = std::max(c->profile_n * c->profile_n, 1);
+    if (A->nprof != np && A->lprof) {
+        cudaFree(A->lprof);
+        A->lprof = nullptr;
+    }
+    ok = ok && alloc((void **)&A->lprof, (size_t)np * sizeof(double));
+    A->nprof = np;
+    if (!ok) {
+        c->err = "adjoint: out of device memory";
+        return PIC_ENOMEM;
+    }
+    return PIC_OK;
+}
+
+template <typename real, int P>
+static void adj_push_launch(pic_ctx *c, AdjState *A, const Blob &b, int kind, int part_base, int scatter) {
+    Species &s = c->sp[kind];
+    AdjPushArgs<real> a{};
+    a.g = c->g;
+    a.cp = c->cp;
+    a.n = b.count[kind];
+    int idx = part_base;
+    if (c->fp32) {
+        a.cell = (const int *)blob_part(b, idx++);
+        a.ox = (const float *)blob_part(b, idx++);
+        a.oy = (const float *)blob_part(b, idx++);
+        a.oz = (const float *)blob_part(b, idx++);
+    } else {
+        a.x = (const double *)blob_part(b, idx++);
+        a.y = (const double *)blob_part(b, idx++);
+        a.z = (const double *)blob_part(b, idx++);
+    }
+    a.px = (const real *)blob_part(b, idx++);
+    a.py = (const real *)blob_part(b, idx++);
+    a.pz = (const real *)blob_part(b, idx++);
+    a.dead = s.dead ? (const unsigned char *)blob_part(b, idx++) : nullptr;
+    const int nparts = (int)b.parts.size();
+    for (int f = 0; f < 6; ++f) a.f[f] = (const real *)blob_part(b, nparts - 6 + f);
+    a.w = (const real *)s.a.w;
+    for (int f = 0; f < 3; ++f) a.lj[f] = (const real *)A->lj[f];
+    for (int f = 0; f < 6; ++f) a.lf[f] = (real *)A->lf[f];
+    real **lp = (real **)A->lpart[kind];
+    a.lx = lp[0]; a.ly = lp[1]; a.lz = lp[2]; a.lpx = lp[3]; a.lpy = lp[4]; a.lpz = lp[5];
+    a.lw = A->lw[kind];
+    const PicParams &p = c->p;
+    a.qm = (real)(p.charge[kind] / p.mass[kind] * p.dt_half);
+    a.charge = (real)p.charge[kind];
+    a.dt_d[0] = (real)(p.dt / p.dx); a.dt_d[1] = (real)(p.dt / p.dy); a.dt_d[2] = (real)(p.dt / p.dz);
+    a.d_dt[0] = p.dx / p.dt; a.d_dt[1] = p.dy / p.dt; a.d_dt[2] = p.dz / p.dt;
+    a.scatter_fields = scatter;
+    a.status = c->d_status;
+    long long blocks = (a.n + 127) / 128;
+    adj_push_kernel<real, P><<<(unsigned)std::min<long long>(blocks, 148 * 16), 128, 0, c->stream>>>(a);
+}
+
+template <typename real>
+static void adj_fields_e(pic_ctx *c, AdjState *A) {
+    const Geom &g = c->g;
+    real **F = (real **)A->lf;
+    real **J = (real **)A->lj;
+    adj_update_e_kernel<real><<<(unsigned)((g.fsz + 255) / 256), 256, 0, c->stream>>>(
+        g, F[0], F[1], F[2], F[3], F[4], F[5], J[0], J[1], J[2], (real)c->p.dt_half, (real)(1.0 / c->p.dx),
+        (real)(1.0 / c->p.dy), (real)(1.0 / c->p.dz));
+}
+
+template <typename real>
+static void adj_fields_b(pic_ctx *c, AdjState *A) {
+    const Geom &g = c->g;
+    real **F = (real **)A->lf;
+    adj_update_b_kernel<real><<<(unsigned)((g.fsz + 255) / 256), 256, 0, c->stream>>>(
+        g, F[0], F[1], F[2], F[3], F[4], F[5], (real)c->p.dt_half, (real)(1.0 / c->p.dx), (real)(1.0 / c->p.dy),
+        (real)(1.0 / c->p.dz));
+}
+
+template <typename real>
+static void adj_bc(pic_ctx *c, AdjState *A, int step) {
+    const Geom &g = c->g;
+    const PicParams &p = c->p;
+    AdjBcArgs B{};
+    B.g = g;
+    B.dt = p.dt; B.dx = p.dx; B.dy = p.dy; B.dz = p.dz;
+    B.Pi = p.Pi; B.omega = p.omega; B.l0 = p.l0; B.amp = p.laser_amplitude; B.dur = p.laser_pulse_duration;
+    B.start = p.laser_start_time; B.waist = p.waist; B.xfocus = p.xfocus; B.yfocus = p.yfocus; B.zfocus = p.zfocus;
+    B.phase = p.phase; B.time = step * p.dt; B.pol = p.laser_polarization; B.envelope = p.laser_envelope;
+    B.profile_n = c->profile_n;
+    B.lprof = (p.laser_profile == 1 && c->d_profile) ? A->lprof : nullptr;
+    real **F = (real **)A->lf;
+    real **J = (real **)A->lj;
+    dim3 blk(32, 8), grd((g.n[1] + 31) / 32, (g.n[2] + 7) / 8);
+    adj_bc_kernel<real><<<grd, blk, 0, c->stream>>>(B, F[0], F[1], F[2], F[3], F[4], F[5], J[1], J[2]);
+}
+
+template <typename real>
+static int adj_backward_t(pic_ctx *c, AdjState *A, int nsteps) {
+    for (int t = 0; t < nsteps; ++t) {
+        if (A->tape_len == 0) {
+            c->err = "adjoint: tape exhausted";
+            return PIC_EINVAL;
+        }
+        const Blob &b = A->tape[--A->tape_len];
+        const int step = b.step;   // 0: the t = 0 push; n >= 1: loop iteration n
+        const bool loop = step >= 1;
+        if (loop) {
+            // second half (field.cpp:88-117): B then E forward, so E then B here
+            adj_fields_e<real>(c, A);
+            adj_fields_b<real>(c, A);
+        }
+        // push + deposit of both species, in reverse species order
+        int base[2] = {0, 0};
+        {
+            int idx = 0;
+            for (int k = 0; k < 2; ++k) {
+                base[k] = idx;
+                if (b.count[k] == 0) continue;
+                idx += (c->fp32 ? 4 : 3) + 3 + (c->sp[k].dead ? 1 : 0);
+            }
+        }
+        for (int k = 1; k >= 0; --k) {
+            if (b.count[k] == 0) continue;
+            if (c->order == 2) adj_push_launch<real, 3>(c, A, b, k, base[k], loop);
+            else adj_push_launch<real, 5>(c, A, b, k, base[k], loop);
+        }
+        // clear_currents: J before the clear does not reach the deposit
+        for (int f = 0; f < 3; ++f) cudaMemsetAsync(A->lj[f], 0, (size_t)c->g.rsz * rsize(c), c->stream);
+        if (loop) {
+            // first half (field.cpp:56-86): E then B forward
+            adj_fields_b<real>(c, A);
+            adj_fields_e<real>(c, A);
+            adj_bc<real>(c, A, step);
+        }
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        c->err = std::string("adjoint: ") + cudaGetErrorString(e);
+        return PIC_ECUDA;
+    }
+    return PIC_OK;
+}
+
+extern "C" {
+
+int pic_checkpoint_save(pic_ctx *c, int slot) {
+    if (!c || slot < 0) return PIC_EINVAL;
+    AdjState *A = adj_of(c, true);
+    if ((int)A->ckpt.size() <= slot) A->ckpt.resize(slot + 1);
+    std::vector<std::pair<void *, size_t>> parts;
+    particle_parts(c, parts);
+    for (int f = 0; f < 6; ++f) parts.push_back({c->field[f], (size_t)c->g.fsz * rsize(c)});
+    for (int f = 0; f < 5; ++f) parts.push_back({c->ring[f], (size_t)c->g.rsz * rsize(c)});
+    return blob_save(c, A->ckpt[slot], parts);
+}
+
+int pic_checkpoint_restore(pic_ctx *c, int slot) {
+    if (!c || slot < 0) return PIC_EINVAL;
+    AdjState *A = adj_of(c, false);
+    if (!A || slot >= (int)A->ckpt.size() || !A->ckpt[slot].buf) {
+        c->err = "no such checkpoint";
+        return PIC_EINVAL;
+    }
+    Blob &b = A->ckpt[slot];
+    for (int k = 0; k < 2; ++k) {
+        if (c->sp[k].n_host != b.count[k]) {
+            c->err = "checkpoint particle count differs from the context's";
+            return PIC_EINVAL;
+        }
+        c->sp[k].cur = b.cur[k];
+    }
+    size_t off = 0;
+    for (auto &p : b.parts) {
+        cudaMemcpyAsync(p.first, (char *)b.buf + off, p.second, cudaMemcpyDeviceToDevice, c->stream);
+        off += (p.second + 255) & ~(size_t)255;
+    }
+    c->step = b.step;
+    return PIC_OK;
+}
+
+int pic_adjoint_tape(pic_ctx *c, int nsteps) {
+    if (!c || nsteps < 0) return PIC_EINVAL;
+    if (!c->p.adjoint) {
+        c->err = "the context was not created with adjoint = 1";
+        return PIC_EINVAL;
+    }
+    AdjState *A = adj_of(c, true);
+    if ((int)A->tape.size() < nsteps) A->tape.resize(nsteps);
+    A->tape_len = 0;
+    return PIC_OK;
+}
+
+int pic_adjoint_record(pic_ctx *c, int on) {
+    if (!c) return PIC_EINVAL;
+    AdjState *A = adj_of(c, true);
+    A->recording = on != 0;
+    return PIC_OK;
+}
+
+int pic_adjoint_seed_kinetic(pic_ctx *c, int kind, double xlo, double xhi, double *loss) {
+    if (!c || kind < 0 || kind > 1) return PIC_EINVAL;
+    if (!c->p.adjoint) {
+        c->err = "the context was not created with adjoint = 1";
+        return PIC_EINVAL;
+    }
+    AdjState *A = adj_of(c, true);
+    int r = ensure_adj_arrays(c, A);
+    if (r) return r;
+    const size_t rs = rsize(c);
+    for (int f = 0; f < 6; ++f) cudaMemsetAsync(A->lf[f], 0, (size_t)c->g.fsz * rs, c->stream);
+    for (int f = 0; f < 3; ++f) cudaMemsetAsync(A->lj[f], 0, (size_t)c->g.rsz * rs, c->stream);
+    for (int k = 0; k < 2; ++k) {
+        size_t n = (size_t)std::max<int64_t>(c->sp[k].cap, 1);
+        for (int q = 0; q < 6; ++q) cudaMemsetAsync(A->lpart[k][q], 0, n * rs, c->stream);
+        cudaMemsetAsync(A->lw[k], 0, n * sizeof(double), c->stream);
+    }
+    cudaMemsetAsync(A->lprof, 0, (size_t)A->nprof * sizeof(double), c->stream);
+    cudaMemsetAsync(A->loss, 0, sizeof(double), c->stream);
+    Species &s = c->sp[kind];
+    long long n = s.n_host;
+    if (n > 0) {
+        unsigned blocks = (unsigned)((n + 255) / 256);
+        if (c->fp32)
+            adj_seed_kinetic_kernel<float><<<blocks, 256, 0, c->stream>>>(
+                c->g, c->cp, 1, n, nullptr, s.a.cell[s.cur], s.a.ox[s.cur], (float *)s.a.px, (float *)s.a.py,
+                (float *)s.a.pz, (float *)s.a.w, s.dead, c->p.mass[kind], xlo, xhi, (float *)A->lpart[kind][3],
+                (float *)A->lpart[kind][4], (float *)A->lpart[kind][5], A->lw[kind], A->loss);
+        else
+            adj_seed_kinetic_kernel<double><<<blocks, 256, 0, c->stream>>>(
+                c->g, c->cp, 0, n, s.a.x[s.cur], nullptr, nullptr, (double *)s.a.px, (double *)s.a.py,
+                (double *)s.a.pz, (double *)s.a.w, s.dead, c->p.mass[kind], xlo, xhi, (double *)A->lpart[kind][3],
+                (double *)A->lpart[kind][4], (double *)A->lpart[kind][5], A->lw[kind], A->loss);
+    }
+    double l = 0.0;
+    cudaMemcpyAsync(&l, A->loss, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return PIC_ECUDA;
+    if (loss) *loss = l;
+    return PIC_OK;
+}
+
+int pic_adjoint_backward(pic_ctx *c, int nsteps) {
+    if (!c || nsteps < 0) return PIC_EINVAL;
+    AdjState *A = adj_of(c, false);
+    if (!A || !A->lf[0]) {
+        c->err = "adjoint: seed the objective first";
+        return PIC_EINVAL;
+    }
+    return c->fp32 ? adj_backward_t<float>(c, A, nsteps) : adj_backward_t<double>(c, A, nsteps);
+}
+
+int pic_adjoint_weight_grad(pic_ctx *c, int kind, double *out, int64_t n) {
+    if (!c || kind < 0 || kind > 1 || !out) return PIC_EINVAL;
+    AdjState *A = adj_of(c, false);
+    if (!A || !A->lw[kind]) return PIC_EINVAL;
+    if (n > c->sp[kind].n_host) n = c->sp[kind].n_host;
+    cudaMemcpyAsync(out, A->lw[kind], (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    return cudaStreamSynchronize(c->stream) == cudaSuccess ? PIC_OK : PIC_ECUDA;
+}
+
+int pic_adjoint_profile_grad(pic_ctx *c, double *out, int n) {
+    if (!c || !out) return PIC_EINVAL;
+    AdjState *A = adj_of(c, false);
+    if (!A || !A->lprof) return PIC_EINVAL;
+    n = std::min(n, A->nprof);
+    cudaMemcpyAsync(out, A->lprof, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    return cudaStreamSynchronize(c->stream) == cudaSuccess ? PIC_OK : PIC_ECUDA;
+}
+
+int pic_adjoint_release(pic_ctx *c) {
+    if (!c) return PIC_EINVAL;
+    for (size_t i = 0; i < g_adj.size(); ++i) {
+        if (g_adj[i].first != c) continue;
+        AdjState *A = g_adj[i].second;
+        for (auto &b : A->ckpt)
+            if (b.buf) cudaFree(b.buf);
+        for (auto &b : A->tape)
+            if (b.buf) cudaFree(b.buf);
+        for (void *p : A->lf) if (p) cudaFree(p);
+        for (void *p : A->lj) if (p) cudaFree(p);
+        for (auto &sp : A->lpart) for (void *p : sp) if (p) cudaFree(p);
+        for (double *p : A->lw) if (p) cudaFree(p);
+        if (A->lprof) cudaFree(A->lprof);
+        if (A->loss) cudaFree(A->loss);
+        delete A;
+        g_adj.erase(g_adj.begin() + (long)i);
+        return PIC_OK;
+    }
+    return PIC_OK;
+}
+
+}  // extern "C"

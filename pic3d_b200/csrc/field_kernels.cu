@@ -244,16 +244,6 @@ struct LaserArgs {
     int is_left, is_right;
 };
 
-__device__ double cubic_bspline(double t) {
-    double a = fabs(t);
-    if (a < 1.0) return (4.0 - 6.0 * a * a + 3.0 * a * a * a) / 6.0;
-    if (a < 2.0) {
-        double b = 2.0 - a;
-        return b * b * b / 6.0;
-    }
-    return 0.0;
-}
-
 __device__ double laser_envelope(const LaserArgs &L, double time, double position) {
     double t = time - position - L.start;
     if (L.envelope == 1) {

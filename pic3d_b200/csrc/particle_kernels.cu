@@ -22,6 +22,7 @@ __global__ void __launch_bounds__(256) push_kernel(PushArgs<real> a) {
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x) {
         const long long p = a.idx ? (long long)a.idx[t] : t;
+        if (a.dead && a.dead[p]) continue;
         OldPos<real> o;
         decode_old(a, p, o);
         if (!in_buffers(a.g, o, H)) {
@@ -179,12 +180,32 @@ __global__ void finish_remove_kernel(long long *count, long long *ctr) {
     *count = *count - ctr[0];
 }
 
+__global__ void mark_dead_kernel(RemoveArgs a, unsigned char *dead) {
+    long long n = *a.count;
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && !dead[i] && is_dead(a, i)) dead[i] = 1;
+}
+
 void launch_remove(pic_ctx *c, int kind) {
     const Geom &g = c->g;
     if (g.per[0] && g.per[1] && g.per[2]) return;
     Species &s = c->sp[kind];
     long long n = s.n_host;
     if (n == 0) return;
+    if (s.dead) {
+        // adjoint mode: particle indices must stay stable across steps
+        RemoveArgs a{};
+        a.g = g;
+        a.cp = c->cp;
+        a.fp32 = c->fp32;
+        a.count = s.d_count;
+        a.x = s.a.x[s.cur]; a.y = s.a.y[s.cur]; a.z = s.a.z[s.cur];
+        a.cell = s.a.cell[s.cur];
+        prof_begin(c, "mark_dead");
+        mark_dead_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(a, s.dead);
+        prof_end(c);
+        return;
+    }
     prof_begin(c, "remove_particles");
     RemoveArgs a{};
     a.g = g;

@@ -67,6 +67,7 @@ void free_species(Species &s) {
     if (s.d_count) cudaFree(s.d_count);
     if (s.keys) cudaFree(s.keys);
     if (s.strag) cudaFree(s.strag);
+    if (s.dead) cudaFree(s.dead);
     if (s.offs) cudaFree(s.offs);
     s = Species{};
 }
@@ -109,11 +110,13 @@ int alloc_species(pic_ctx *c, int kind, int64_t cap, bool spin) {
         r = r ? r : dalloc(c, &s.offs, (size_t)(c->nkeys + 1) * sizeof(unsigned));
     }
     r = r ? r : dalloc(c, &s.d_count, sizeof(long long));
+    if (c->p.adjoint && cap > 0) r = r ? r : dalloc(c, &s.dead, n);
     if (r != PIC_OK) {
         free_species(s);
         return r;
     }
     cudaMemsetAsync(s.d_count, 0, sizeof(long long), c->stream);
+    if (s.dead) cudaMemsetAsync(s.dead, 0, n, c->stream);
     return PIC_OK;
 }
 
@@ -280,6 +283,13 @@ int pic_create(const PicParams *pp, int device, pic_ctx **out) {
     if (c->fp32 && c->cp.bx + c->cp.by + c->cp.bz > 31) return bad("grid too large for the packed int32 cell index");
     // tiling: 0 -> default edge of 4 cells, < 0 -> global-memory kernel only
     c->tile = p.tile == 0 ? 4 : (p.tile < 0 ? 0 : p.tile);
+    if (p.adjoint) {
+        // per-particle adjoints need particle indices that never change:
+        // no sorting, removal only marks particles dead
+        if (p.rank_period[0] || p.rank_period[1] || p.rank_period[2])
+            return bad("the adjoint supports absorbing faces only");
+        c->tile = 0;
+    }
     c->sort_interval = p.sort_interval > 0 ? p.sort_interval : 4;
     if (c->tile > 0) {
         for (int d = 0; d < 3; ++d) c->ntile[d] = (n[d] + c->tile - 1) / c->tile;
@@ -339,6 +349,7 @@ int pic_destroy(pic_ctx *c) {
     if (!c) return PIC_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    pic_adjoint_release(c);
     for (auto &e : c->prof_events) {
         cudaEventDestroy(e.a);
         cudaEventDestroy(e.b);
@@ -432,6 +443,7 @@ int pic_upload_particles(pic_ctx *c, int kind, const void *records, int64_t n) {
     }
     s.cur = 0;
     s.sorted = false;
+    if (s.dead) cudaMemsetAsync(s.dead, 0, (size_t)s.cap, c->stream);
     s.spin_nonzero = spin_nonzero;
     s.max_abs_w = wmax;
     int r = ensure_stage(c, (size_t)(n < kChunk ? n : kChunk) * 144);
@@ -576,6 +588,7 @@ int pic_exchange_currents(pic_ctx *c) {
 int pic_initial_push(pic_ctx *c) {
     if (!c) return PIC_EINVAL;
     int r;
+    adjoint_record_hook(c);
     if ((r = push_both(c))) return r;
     if ((r = pic_exchange_particles(c, 0))) return r;
     return pic_exchange_particles(c, 1);
@@ -590,6 +603,7 @@ int pic_run_steps(pic_ctx *c, int nsteps) {
         if ((r = pic_radiating_boundary(c, 1, 0, c->step))) return r;
         if ((r = pic_update_fields_first(c))) return r;
         if ((r = pic_clear_currents(c))) return r;
+        adjoint_record_hook(c);
         if ((r = push_both(c))) return r;
         if ((r = pic_exchange_particles(c, 0))) return r;
         if ((r = pic_exchange_particles(c, 1))) return r;

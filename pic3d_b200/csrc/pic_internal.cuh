@@ -78,6 +78,17 @@ __device__ __forceinline__ void shape_weights(real d, real (&w)[5]) {
     w[4] = u2 * u2 * real(1.0 / 24.0);
 }
 
+// cubic B-spline basis of the laser amplitude grid (extension), support |t| < 2
+__device__ __forceinline__ double cubic_bspline(double t) {
+    double a = fabs(t);
+    if (a < 1.0) return (4.0 - 6.0 * a * a + 3.0 * a * a * a) / 6.0;
+    if (a < 2.0) {
+        double b = 2.0 - a;
+        return b * b * b / 6.0;
+    }
+    return 0.0;
+}
+
 // ---------------------------------------------------------------------------
 // particle storage (structure of arrays, one set per species)
 //   FP64: x,y,z absolute cell coordinates as in the reference, two buffers
@@ -101,6 +112,7 @@ struct Species {
     PartArrays b;            // destination of the counting sort (same shapes)
     int *keys = nullptr;     // per-particle sort key
     int *strag = nullptr;    // particles the tiled kernel hands to the global kernel
+    unsigned char *dead = nullptr;  // adjoint mode: 1 once a particle left through an absorbing face
     unsigned *offs = nullptr;  // per-key start offsets after the last sort (nkeys + 1)
     bool sorted = false;     // offs describes the current order
     int pushes_since_sort = 0;

@@ -28,6 +28,9 @@ void launch_sort(pic_ctx *c, int kind);
 void launch_tile_push(pic_ctx *c, int mask);
 size_t tile_smem_bytes(const pic_ctx *c);
 
+// adjoint_kernels.cu
+void adjoint_record_hook(pic_ctx *c);
+
 // diag_kernels.cu
 void launch_diagnostics(pic_ctx *c, double *d_out);
 

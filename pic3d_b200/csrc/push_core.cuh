@@ -18,6 +18,7 @@ struct PushArgs {
     real *jx, *jy, *jz, *rho;
     const long long *count;
     const int *idx;          // optional list of particle indices (count entries); null: all particles
+    const unsigned char *dead;   // adjoint mode: particles already removed are skipped (null otherwise)
     // FP64 positions (cur -> nxt)
     double *x0, *y0, *z0;
     double *x1, *y1, *z1;
@@ -521,6 +522,7 @@ inline PushArgs<real> make_push_args(pic_ctx *c, int kind) {
     a.E_schwinger = p.E_schwinger; a.dt_half_d = p.dt_half; a.charge_d = p.charge[kind]; a.mass_d = p.mass[kind];
     a.electron = spin_active(c, kind) ? 1 : 0;
     a.status = c->d_status;
+    a.dead = s.dead;
     return a;
 }
 

@@ -19,7 +19,8 @@ from .workloads import PARTICLE_DTYPE, Workload
 
 
 def params_from(w, precision: str | None = None, spin: bool = True, deposit_rho: bool = True,
-                capacity=(0, 0), laser_profile: bool = False, tile: int = 0, sort_interval: int = 0) -> L.PicParams:
+                capacity=(0, 0), laser_profile: bool = False, tile: int = 0, sort_interval: int = 0,
+                adjoint: bool = False) -> L.PicParams:
     """PicParams from a Workload or a reference parameter dictionary."""
     p = w if isinstance(w, dict) else w.params()
     prec = precision or (w.precision if isinstance(w, Workload) else "fp64")
@@ -43,6 +44,7 @@ def params_from(w, precision: str | None = None, spin: bool = True, deposit_rho:
     pp.capacity[0], pp.capacity[1] = int(capacity[0]), int(capacity[1])
     pp.tile = int(tile)
     pp.sort_interval = int(sort_interval)
+    pp.adjoint = 1 if adjoint else 0
     pp.charge[0], pp.mass[0] = -1.0, 1.0
     pp.charge[1], pp.mass[1] = 1.0, 1836.0
     return pp
@@ -53,12 +55,12 @@ class Simulation:
 
     def __init__(self, w, precision: str | None = None, device: int = 0, spin: bool = True,
                  deposit_rho: bool = True, capacity=(0, 0), laser_profile=None, tile: int = 0,
-                 sort_interval: int = 0):
+                 sort_interval: int = 0, adjoint: bool = False):
         """tile: edge of the shared-memory particle tile in cells (0 default,
         -1 global-memory kernel); sort_interval: pushes between sorts."""
         self.lib = L.load()
         self.params = params_from(w, precision, spin, deposit_rho, capacity, laser_profile is not None, tile,
-                                  sort_interval)
+                                  sort_interval, adjoint)
         self.w = w
         h = ctypes.c_void_p()
         self._check(self.lib.pic_create(ctypes.byref(self.params), device, ctypes.byref(h)), None)

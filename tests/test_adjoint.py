@@ -1,0 +1,96 @@
+"""The hand-written adjoint against central finite differences.
+
+A small laser run (absorbing faces, electrons with a small thermal spread,
+laser amplitude from a 4x4 B-spline coefficient grid) is differentiated with
+respect to the density knots and the laser coefficients; the objective is
+the electrons' kinetic energy in a window at the final step.  Finite
+differences use the FP64 forward run.
+"""
+import numpy as np
+import pytest
+
+from pic3d_b200.workloads import LAMBDA, Workload
+
+pytestmark = pytest.mark.gpu
+
+
+def small_spec(precision="fp64", mem=2, segment=5, steps=16):
+    from pic3d_b200.adjoint import AdjointSpec
+    w = Workload(name="adj_small", nx=24, ny=12, nz=12, mem=mem, period=(0, 0, 0), dx=LAMBDA / 16, dy=LAMBDA / 8,
+                 dz=LAMBDA / 8, ppc=(2, 0), u_th=(0.02, 0.0), laser_amplitude=1.0, laser_pulse_duration=4.0,
+                 waist=LAMBDA, laser_polarization=3, steps=steps)
+    return AdjointSpec(workload=w, n_knots=6, profile_n=4, window=(2.0, 20.0), segment=segment, seed=77,
+                       precision=precision)
+
+
+def params(spec):
+    rng = np.random.default_rng(5)
+    knots = 0.05 + 0.05 * rng.random(spec.n_knots)
+    prof = 1.0 + 0.5 * rng.random((spec.profile_n, spec.profile_n))
+    return knots, prof
+
+
+def fd(spec, knots, prof, which, idx, h):
+    from pic3d_b200.adjoint import objective
+    k1, p1 = knots.copy(), prof.copy().ravel()
+    k2, p2 = knots.copy(), prof.copy().ravel()
+    if which == "knot":
+        k1[idx] += h
+        k2[idx] -= h
+    else:
+        p1[idx] += h
+        p2[idx] -= h
+    return (objective(spec, k1, p1) - objective(spec, k2, p2)) / (2 * h)
+
+
+@pytest.mark.parametrize("mem", [2, 4])
+def test_adjoint_matches_finite_differences(mem):
+    from pic3d_b200.adjoint import objective_and_grad
+    spec = small_spec("fp64", mem=mem)
+    knots, prof = params(spec)
+    loss, gk, gp, _ = objective_and_grad(spec, knots, prof)
+    assert loss > 0
+    assert np.abs(gp).max() > 0, "laser coefficients must influence the objective"
+    scale_k = np.abs(gk).max()
+    for i in range(spec.n_knots):
+        f = fd(spec, knots, prof, "knot", i, 1e-5)
+        assert abs(gk[i] - f) <= 1e-4 * max(abs(f), 1e-3 * scale_k), (i, gk[i], f)
+    scale_p = np.abs(gp).max()
+    for i in [0, 5, 6, 9, 10, 15]:
+        f = fd(spec, knots, prof, "prof", i, 1e-4)
+        assert abs(gp[i] - f) <= 1e-4 * max(abs(f), 1e-2 * scale_p), (i, gp[i], f)
+
+
+def test_segments_do_not_change_the_gradient():
+    from pic3d_b200.adjoint import objective_and_grad
+    knots, prof = params(small_spec())
+    a = objective_and_grad(small_spec(segment=3), knots, prof)
+    b = objective_and_grad(small_spec(segment=100), knots, prof)
+    assert a[0] == pytest.approx(b[0], rel=1e-12)
+    np.testing.assert_allclose(a[1], b[1], rtol=1e-9, atol=1e-14)
+    np.testing.assert_allclose(a[2], b[2], rtol=1e-9, atol=1e-14)
+
+
+def test_fp32_adjoint_matches_fp64():
+    from pic3d_b200.adjoint import objective_and_grad
+    knots, prof = params(small_spec())
+    l64, k64, p64, _ = objective_and_grad(small_spec("fp64"), knots, prof)
+    l32, k32, p32, _ = objective_and_grad(small_spec("fp32"), knots, prof)
+    assert l32 == pytest.approx(l64, rel=1e-5)
+    assert np.linalg.norm(k32 - k64) <= 1e-4 * np.linalg.norm(k64)
+    assert np.linalg.norm(p32 - p64) <= 1e-3 * np.linalg.norm(p64)
+
+
+def test_autograd_function():
+    import torch
+
+    from pic3d_b200.adjoint import PICObjective, objective_and_grad
+    spec = small_spec()
+    knots, prof = params(spec)
+    kt = torch.tensor(knots, requires_grad=True)
+    pt = torch.tensor(prof.ravel(), requires_grad=True)
+    loss = PICObjective.apply(kt, pt, spec)
+    (2.0 * loss).backward()
+    _, gk, gp, _ = objective_and_grad(spec, knots, prof)
+    np.testing.assert_allclose(kt.grad.numpy(), 2.0 * gk, rtol=1e-9)
+    np.testing.assert_allclose(pt.grad.numpy(), 2.0 * gp, rtol=1e-9)
