@@ -241,6 +241,67 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def adjoint_bench(steps=600, fd_params=2):
+    """Differentiable run: forward (with checkpoints every 50 steps) and
+    adjoint (segment recompute + reverse sweep) in FP32, the same gradient
+    in FP64, and central finite differences of the FP64 forward run."""
+    import numpy as np
+
+    from pic3d_b200 import workloads as W
+    from pic3d_b200.adjoint import AdjointRun, AdjointSpec, objective
+
+    def spec(prec):
+        w = W.differentiable_laser(precision=prec, steps=steps)
+        return AdjointSpec(workload=w, n_knots=32, profile_n=8, window=(0.75 * w.nx, float(w.nx)), segment=50,
+                           seed=2468, precision=prec)
+
+    rng = np.random.default_rng(13)
+    knots = 0.01 + 0.02 * rng.random(32)
+    prof = 1.0 + 0.2 * rng.random((8, 8))
+    out = {}
+    for prec in ("fp32", "fp64"):
+        sp = spec(prec)
+        run = AdjointRun(sp, knots, prof)
+        run.sim.synchronize()
+        t0 = time.perf_counter()
+        loss = run.forward()
+        run.sim.synchronize()
+        t1 = time.perf_counter()
+        gw, gp = run.backward()
+        run.sim.synchronize()
+        t2 = time.perf_counter()
+        gk = sp.knot_grad(run.x0, gw)
+        out[prec] = dict(loss=loss, gk=gk, gp=gp, fwd=t1 - t0, bwd=t2 - t1, n=len(run.records))
+        run.close()
+    a, b = out["fp32"], out["fp64"]
+    rel = lambda x, y: float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+    sp64 = spec("fp64")
+    checks = []
+    for which, idx in [("knot", int(np.argmax(np.abs(b["gk"])))), ("laser", int(np.argmax(np.abs(b["gp"]))))][:fd_params]:
+        k1, k2, p1, p2 = knots.copy(), knots.copy(), prof.ravel().copy(), prof.ravel().copy()
+        if which == "knot":
+            h = 1e-4 * abs(knots[idx])
+            k1[idx] += h
+            k2[idx] -= h
+            g = b["gk"][idx]
+        else:
+            h = 1e-4 * abs(prof.ravel()[idx])
+            p1[idx] += h
+            p2[idx] -= h
+            g = b["gp"][idx]
+        f = (objective(sp64, k1, p1) - objective(sp64, k2, p2)) / (2 * h)
+        checks.append({"param": f"{which}[{idx}]", "adjoint_fp64": g, "central_fd_fp64": f,
+                       "rel_err": abs(g - f) / max(abs(f), 1e-300)})
+    return {"workload": spec("fp32").workload.name, "particles": a["n"], "steps": steps, "checkpoint_every": 50,
+            "parameters": 32 + 64, "objective_fp32": a["loss"], "objective_fp64": b["loss"],
+            "forward_s": a["fwd"], "adjoint_s": a["bwd"], "adjoint_over_forward": a["bwd"] / a["fwd"],
+            "fp64_forward_s": b["fwd"], "fp64_adjoint_s": b["bwd"],
+            "grad_rel_l2_fp32_vs_fp64": {"knots": rel(a["gk"], b["gk"]), "laser": rel(a["gp"], b["gp"])},
+            "finite_difference_checks": checks,
+            "note": "adjoint = restore each checkpoint, recompute its 50 steps recording the push inputs, reverse "
+                    "sweep; forward = the run with checkpoints; both in adjoint mode (global push kernel)"}
+
+
 def field_rel_err(a: dict, b: dict):
     num = sum(float(np.sum((a[n] - b[n]) ** 2)) for n in ("ex", "ey", "ez", "bx", "by", "bz"))
     den = sum(float(np.sum(b[n] ** 2)) for n in ("ex", "ey", "ez", "bx", "by", "bz"))
@@ -258,6 +319,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-steps", type=int, default=600)
     ap.add_argument("--tile", type=int, default=0, help="shared-memory tile edge (0 default, -1 global kernel)")
     ap.add_argument("--sort-interval", type=int, default=0)
     args = ap.parse_args()
@@ -386,6 +449,12 @@ def main():
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "note": "pic_upload_* of the initial state from host memory, the t=0 push, K pic_run_steps(1) "
                        "each followed by a pic_diagnostics read-back, pic_download_* of the final state"}
+
+    if rank == 0 and not args.no_adjoint:
+        try:
+            extra["adjoint"] = adjoint_bench(args.adjoint_steps)
+        except Exception as e:
+            extra["adjoint"] = {"error": str(e)[:300]}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

@@ -203,10 +203,23 @@ def thermal_scaleup(nx=512, ny=256, nz=256, mem=2, precision="fp32", steps=100) 
                     steps=steps, precision=precision)
 
 
+def differentiable_laser(nx=64, ny=64, nz=128, precision="fp32", steps=600, mem=4) -> Workload:
+    """Differentiable run: 64 x 64 x 128 cells (dx = dy = dz = lambda/16),
+    electrons at 8 per cell (weights from a 32-knot density profile set by
+    the caller), a laser from x-min whose transverse amplitude is an 8 x 8
+    cubic-B-spline coefficient grid (a0 about 1), absorbing faces, 600
+    steps."""
+    return Workload(name=f"differentiable_laser_{nx}x{ny}x{nz}_{precision}", nx=nx, ny=ny, nz=nz, mem=mem,
+                    period=(0, 0, 0), dx=LAMBDA / 16, dy=LAMBDA / 16, dz=LAMBDA / 16, ppc=(8, 0), u_th=(0.0, 0.0),
+                    density_value=0.02, laser_amplitude=1.0, laser_pulse_duration=10.0 * LAMBDA,
+                    waist=2.0 * LAMBDA, laser_polarization=1, steps=steps, precision=precision)
+
+
 WORKLOADS = {
     "thermal_periodic": thermal_periodic,
     "laser_underdense": laser_underdense,
     "thermal_scaleup": thermal_scaleup,
+    "differentiable_laser": differentiable_laser,
 }
 
 
