@@ -241,26 +241,35 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
-def adjoint_bench(steps=600, fd_params=2):
+def adjoint_bench(steps=600, short_steps=100):
     """Differentiable run: forward (with checkpoints every 50 steps) and
-    adjoint (segment recompute + reverse sweep) in FP32, the same gradient
-    in FP64, and central finite differences of the FP64 forward run."""
+    adjoint (segment recompute + reverse sweep) in FP32, the same gradient in
+    FP64, and central finite differences of the FP64 forward run at a
+    sequence of steps.
+
+    The objective is only piecewise smooth: electrons leave through the
+    absorbing faces (hundreds of thousands per 100 steps here) and each
+    removal is a jump, so differences converge to the derivative only once
+    the step is small enough that no removal changes step (about 1e-8 of the
+    parameter at 600 steps).  The same roughness makes the FP32 and FP64
+    derivatives differ at long horizons (the FP32 trajectory differs from the
+    FP64 one by more than that scale); the FP32 / FP64 agreement is also
+    reported at a short horizon where it is not rough."""
     import numpy as np
 
     from pic3d_b200 import workloads as W
     from pic3d_b200.adjoint import AdjointRun, AdjointSpec, objective
 
-    def spec(prec):
-        w = W.differentiable_laser(precision=prec, steps=steps)
-        return AdjointSpec(workload=w, n_knots=32, profile_n=8, window=(0.75 * w.nx, float(w.nx)), segment=50,
-                           seed=2468, precision=prec)
+    def spec(prec, n=steps):
+        w = W.differentiable_laser(precision=prec, steps=n)
+        return AdjointSpec(workload=w, n_knots=32, profile_n=8, window=(0.5 * w.nx, w.nx - 4.0), ramp=4.0,
+                           segment=50, seed=2468, precision=prec)
 
     rng = np.random.default_rng(13)
     knots = 0.01 + 0.02 * rng.random(32)
     prof = 1.0 + 0.2 * rng.random((8, 8))
-    out = {}
-    for prec in ("fp32", "fp64"):
-        sp = spec(prec)
+
+    def grad(sp):
         run = AdjointRun(sp, knots, prof)
         run.sim.synchronize()
         t0 = time.perf_counter()
@@ -271,35 +280,45 @@ def adjoint_bench(steps=600, fd_params=2):
         run.sim.synchronize()
         t2 = time.perf_counter()
         gk = sp.knot_grad(run.x0, gw)
-        out[prec] = dict(loss=loss, gk=gk, gp=gp, fwd=t1 - t0, bwd=t2 - t1, n=len(run.records))
+        n = len(run.records)
         run.close()
-    a, b = out["fp32"], out["fp64"]
+        return dict(loss=loss, gk=gk, gp=gp, fwd=t1 - t0, bwd=t2 - t1, n=n)
+
     rel = lambda x, y: float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+    a, b = grad(spec("fp32")), grad(spec("fp64"))
+    sa, sb = grad(spec("fp32", short_steps)), grad(spec("fp64", short_steps))
     sp64 = spec("fp64")
     checks = []
-    for which, idx in [("knot", int(np.argmax(np.abs(b["gk"])))), ("laser", int(np.argmax(np.abs(b["gp"]))))][:fd_params]:
-        k1, k2, p1, p2 = knots.copy(), knots.copy(), prof.ravel().copy(), prof.ravel().copy()
-        if which == "knot":
-            h = 1e-4 * abs(knots[idx])
-            k1[idx] += h
-            k2[idx] -= h
-            g = b["gk"][idx]
-        else:
-            h = 1e-4 * abs(prof.ravel()[idx])
-            p1[idx] += h
-            p2[idx] -= h
-            g = b["gp"][idx]
-        f = (objective(sp64, k1, p1) - objective(sp64, k2, p2)) / (2 * h)
-        checks.append({"param": f"{which}[{idx}]", "adjoint_fp64": g, "central_fd_fp64": f,
-                       "rel_err": abs(g - f) / max(abs(f), 1e-300)})
+    for which, idx in [("knot", int(np.argmax(np.abs(b["gk"])))), ("laser", int(np.argmax(np.abs(b["gp"]))))]:
+        g = b["gk"][idx] if which == "knot" else b["gp"][idx]
+        base = knots[idx] if which == "knot" else prof.ravel()[idx]
+        fds = {}
+        for rel_h in (1e-5, 1e-8, 1e-9):
+            k1, k2, p1, p2 = knots.copy(), knots.copy(), prof.ravel().copy(), prof.ravel().copy()
+            h = rel_h * abs(base)
+            if which == "knot":
+                k1[idx] += h
+                k2[idx] -= h
+            else:
+                p1[idx] += h
+                p2[idx] -= h
+            fds[f"{rel_h:g}"] = (objective(sp64, k1, p1) - objective(sp64, k2, p2)) / (2 * h)
+        checks.append({"param": f"{which}[{idx}]", "adjoint_fp64": g, "central_fd_fp64_by_relative_step": fds,
+                       "rel_err_by_relative_step": {k: abs(g - f) / max(abs(f), 1e-300) for k, f in fds.items()}})
     return {"workload": spec("fp32").workload.name, "particles": a["n"], "steps": steps, "checkpoint_every": 50,
-            "parameters": 32 + 64, "objective_fp32": a["loss"], "objective_fp64": b["loss"],
+            "parameters": 32 + 64, "objective": "sum s(x) w m (gamma-1), s = 1 on x in [32, 60) cells with 4-cell "
+                                                  "sin^2 ramps",
+            "objective_fp32": a["loss"], "objective_fp64": b["loss"],
             "forward_s": a["fwd"], "adjoint_s": a["bwd"], "adjoint_over_forward": a["bwd"] / a["fwd"],
             "fp64_forward_s": b["fwd"], "fp64_adjoint_s": b["bwd"],
             "grad_rel_l2_fp32_vs_fp64": {"knots": rel(a["gk"], b["gk"]), "laser": rel(a["gp"], b["gp"])},
+            f"grad_rel_l2_fp32_vs_fp64_{short_steps}_steps": {"knots": rel(sa["gk"], sb["gk"]),
+                                                              "laser": rel(sa["gp"], sb["gp"])},
             "finite_difference_checks": checks,
             "note": "adjoint = restore each checkpoint, recompute its 50 steps recording the push inputs, reverse "
-                    "sweep; forward = the run with checkpoints; both in adjoint mode (global push kernel)"}
+                    "sweep; forward = the run with checkpoints; both in adjoint mode (global push kernel); central "
+                    "differences of a piecewise-smooth objective converge only at small steps (particle removal "
+                    "at the absorbing faces)"}
 
 
 def field_rel_err(a: dict, b: dict):

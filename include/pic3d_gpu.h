@@ -179,9 +179,12 @@ int pic_field_diagnostics_noalloc(const PicParams *p, const double *ex, const do
  *   pic_checkpoint_save/restore   device copies of the whole state
  *   pic_adjoint_tape(n) + pic_adjoint_record(1), then pic_initial_push /
  *   pic_run_steps re-run a segment recording each push's inputs
- *   pic_adjoint_seed_kinetic      objective = sum w m (gamma-1) of one
- *                                 species' particles with x in [xlo, xhi)
- *                                 at the current state; zeroes all adjoints
+ *   pic_adjoint_seed_kinetic      objective = sum s(x) w m (gamma-1) over
+ *                                 one species' particles at the current
+ *                                 state, s = 1 inside [xlo, xhi), 0 outside,
+ *                                 sin^2 ramps `ramp` cells wide at both
+ *                                 ends (ramp 0: hard edges, not smooth in
+ *                                 x); zeroes all adjoints
  *   pic_adjoint_backward(n)       n recorded steps in reverse
  *   pic_adjoint_weight_grad       d objective / d weight, per particle in
  *                                 upload order
@@ -190,7 +193,7 @@ int pic_checkpoint_save(pic_ctx *ctx, int slot);
 int pic_checkpoint_restore(pic_ctx *ctx, int slot);
 int pic_adjoint_tape(pic_ctx *ctx, int nsteps);
 int pic_adjoint_record(pic_ctx *ctx, int on);
-int pic_adjoint_seed_kinetic(pic_ctx *ctx, int kind, double xlo, double xhi, double *objective);
+int pic_adjoint_seed_kinetic(pic_ctx *ctx, int kind, double xlo, double xhi, double ramp, double *objective);
 int pic_adjoint_backward(pic_ctx *ctx, int nsteps);
 int pic_adjoint_weight_grad(pic_ctx *ctx, int kind, double *grad, int64_t n);
 int pic_adjoint_profile_grad(pic_ctx *ctx, double *grad, int n);

@@ -99,7 +99,7 @@ def load(path: str = LIB_PATH):
     lib.pic_checkpoint_restore.argtypes = [V, ctypes.c_int]
     lib.pic_adjoint_tape.argtypes = [V, ctypes.c_int]
     lib.pic_adjoint_record.argtypes = [V, ctypes.c_int]
-    lib.pic_adjoint_seed_kinetic.argtypes = [V, ctypes.c_int, _D, _D, P(_D)]
+    lib.pic_adjoint_seed_kinetic.argtypes = [V, ctypes.c_int, _D, _D, _D, P(_D)]
     lib.pic_adjoint_backward.argtypes = [V, ctypes.c_int]
     lib.pic_adjoint_weight_grad.argtypes = [V, ctypes.c_int, V, _I64]
     lib.pic_adjoint_profile_grad.argtypes = [V, V, ctypes.c_int]

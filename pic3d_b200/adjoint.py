@@ -1,7 +1,9 @@
 """Gradients of a final-state objective through the PIC loop.
 
-The objective is the kinetic energy sum w m (gamma - 1) of the electrons
-whose x lies in a window at the final step.  The parameters are
+The objective is the kinetic energy sum s(x) w m (gamma - 1) of the
+electrons at the final step, s a window along x (1 inside, 0 outside, with
+sin^2 ramps `ramp` cells wide at its edges so that the objective is smooth
+in the particle positions).  The parameters are
   * K density knots: the initial density is the piecewise-linear
     interpolation of the knot values along x, and each particle's weight is
     density(x0) / (particles per cell) at its initial position;
@@ -40,6 +42,7 @@ class AdjointSpec:
     n_knots: int = 32
     profile_n: int = 8
     window: tuple = (0.0, 0.0)        # x range of the objective, in cells
+    ramp: float = 0.0                 # width of the window's edge ramps, in cells
     segment: int = 50
     seed: int = 4321
     precision: str = "fp32"
@@ -104,7 +107,8 @@ class AdjointRun:
             self.bounds.append((0, 0, 0, True))
         loss = ctypes.c_double()
         self._ck(self.lib.pic_adjoint_seed_kinetic(self.ctx, 0, float(self.spec.window[0]),
-                                                   float(self.spec.window[1]), ctypes.byref(loss)))
+                                                   float(self.spec.window[1]), float(self.spec.ramp),
+                                                   ctypes.byref(loss)))
         return loss.value
 
     def backward(self):

@@ -640,13 +640,38 @@ __global__ void adj_bc_kernel(AdjBcArgs A, real *lex, real *ley, real *lez, real
     }
 }
 
-// objective: kinetic energy sum w m (gamma - 1) of the alive particles of a
-// species with x in [xlo, xhi); seeds d objective / d p and / d w
+// smooth window over [xlo, xhi): 0 outside, 1 inside, sin^2 ramps of width
+// `ramp` cells at both ends (ramp = 0: a hard window); returns s(x), ds/dx
+__device__ inline void window_weight(double x, double xlo, double xhi, double ramp, double &s, double &ds) {
+    s = 0.0;
+    ds = 0.0;
+    if (!(x >= xlo && x < xhi)) return;
+    const double half_pi = 1.5707963267948966;
+    s = 1.0;
+    if (ramp > 0.0) {
+        const double up = (x - xlo) / ramp, down = (xhi - x) / ramp;
+        if (up < 1.0) {
+            double sn = sin(half_pi * up), cs = cos(half_pi * up);
+            s = sn * sn;
+            ds = 2.0 * sn * cs * half_pi / ramp;
+        }
+        if (down < 1.0) {
+            double sn = sin(half_pi * down), cs = cos(half_pi * down);
+            double s2 = sn * sn, d2 = -2.0 * sn * cs * half_pi / ramp;
+            ds = ds * s2 + s * d2;
+            s *= s2;
+        }
+    }
+}
+
+// objective: kinetic energy sum s(x) w m (gamma - 1) of the alive particles
+// of a species, s the window weight above; seeds d objective / d (x, p, w)
 template <typename real>
 __global__ void adj_seed_kinetic_kernel(Geom g, CellPack cp, int fp32, long long n, const double *x, const int *cell,
                                         const float *ox, const real *px, const real *py, const real *pz,
                                         const real *w, const unsigned char *dead, double mass, double xlo,
-                                        double xhi, real *lpx, real *lpy, real *lpz, double *lw, double *loss) {
+                                        double xhi, double ramp, real *lx, real *lpx, real *lpy, real *lpz,
+                                        double *lw, double *loss) {
     long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double contrib = 0.0;
     if (p < n && !(dead && dead[p])) {
@@ -658,16 +683,19 @@ __global__ void adj_seed_kinetic_kernel(Geom g, CellPack cp, int fp32, long long
         } else {
             xp = x[p];
         }
-        if (xp >= xlo && xp < xhi) {
+        double sw, dsw;
+        window_weight(xp, xlo, xhi, ramp, sw, dsw);
+        if (sw != 0.0) {
             double a = px[p], b = py[p], c = pz[p];
             double u2 = a * a + b * b + c * c, gam = sqrt(1.0 + u2);
             double gm1 = u2 / (gam + 1.0);
             double wt = w[p];
-            contrib = wt * mass * gm1;
-            lpx[p] += (real)(wt * mass * a / gam);
-            lpy[p] += (real)(wt * mass * b / gam);
-            lpz[p] += (real)(wt * mass * c / gam);
-            lw[p] += mass * gm1;
+            contrib = sw * wt * mass * gm1;
+            lx[p] += (real)(dsw * wt * mass * gm1);
+            lpx[p] += (real)(sw * wt * mass * a / gam);
+            lpy[p] += (real)(sw * wt * mass * b / gam);
+            lpz[p] += (real)(sw * wt * mass * c / gam);
+            lw[p] += sw * mass * gm1;
         }
     }
     // warp reduction of the loss
@@ -1003,8 +1031,11 @@ int pic_adjoint_record(pic_ctx *c, int on) {
     return PIC_OK;
 }
 
-int pic_adjoint_seed_kinetic(pic_ctx *c, int kind, double xlo, double xhi, double *loss) {
-    if (!c || kind < 0 || kind > 1) return PIC_EINVAL;
+int pic_adjoint_seed_kinetic(pic_ctx *c, int kind, double xlo, double xhi, double ramp, double *loss) {
+    if (!c || kind < 0 || kind > 1 || !(ramp >= 0.0) || !(xhi >= xlo) || 2.0 * ramp > xhi - xlo) {
+        if (c) c->err = "adjoint: window needs xlo <= xhi and 0 <= 2 ramp <= xhi - xlo";
+        return PIC_EINVAL;
+    }
     if (!c->p.adjoint) {
         c->err = "the context was not created with adjoint = 1";
         return PIC_EINVAL;
@@ -1029,12 +1060,12 @@ int pic_adjoint_seed_kinetic(pic_ctx *c, int kind, double xlo, double xhi, doubl
         if (c->fp32)
             adj_seed_kinetic_kernel<float><<<blocks, 256, 0, c->stream>>>(
                 c->g, c->cp, 1, n, nullptr, s.a.cell[s.cur], s.a.ox[s.cur], (float *)s.a.px, (float *)s.a.py,
-                (float *)s.a.pz, (float *)s.a.w, s.dead, c->p.mass[kind], xlo, xhi, (float *)A->lpart[kind][3],
+                (float *)s.a.pz, (float *)s.a.w, s.dead, c->p.mass[kind], xlo, xhi, ramp, (float *)A->lpart[kind][0], (float *)A->lpart[kind][3],
                 (float *)A->lpart[kind][4], (float *)A->lpart[kind][5], A->lw[kind], A->loss);
         else
             adj_seed_kinetic_kernel<double><<<blocks, 256, 0, c->stream>>>(
                 c->g, c->cp, 0, n, s.a.x[s.cur], nullptr, nullptr, (double *)s.a.px, (double *)s.a.py,
-                (double *)s.a.pz, (double *)s.a.w, s.dead, c->p.mass[kind], xlo, xhi, (double *)A->lpart[kind][3],
+                (double *)s.a.pz, (double *)s.a.w, s.dead, c->p.mass[kind], xlo, xhi, ramp, (double *)A->lpart[kind][0], (double *)A->lpart[kind][3],
                 (double *)A->lpart[kind][4], (double *)A->lpart[kind][5], A->lw[kind], A->loss);
     }
     double l = 0.0;

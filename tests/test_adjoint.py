@@ -14,10 +14,10 @@ from pic3d_b200.workloads import LAMBDA, Workload
 pytestmark = pytest.mark.gpu
 
 
-def small_spec(precision="fp64", mem=2, segment=5, steps=16):
+def small_spec(precision="fp64", mem=2, segment=5, steps=16, u_th=0.02):
     from pic3d_b200.adjoint import AdjointSpec
     w = Workload(name="adj_small", nx=24, ny=12, nz=12, mem=mem, period=(0, 0, 0), dx=LAMBDA / 16, dy=LAMBDA / 8,
-                 dz=LAMBDA / 8, ppc=(2, 0), u_th=(0.02, 0.0), laser_amplitude=1.0, laser_pulse_duration=4.0,
+                 dz=LAMBDA / 8, ppc=(2, 0), u_th=(u_th, 0.0), laser_amplitude=1.0, laser_pulse_duration=4.0,
                  waist=LAMBDA, laser_polarization=3, steps=steps)
     return AdjointSpec(workload=w, n_knots=6, profile_n=4, window=(2.0, 20.0), segment=segment, seed=77,
                        precision=precision)
@@ -59,6 +59,57 @@ def test_adjoint_matches_finite_differences(mem):
     for i in [0, 5, 6, 9, 10, 15]:
         f = fd(spec, knots, prof, "prof", i, 1e-4)
         assert abs(gp[i] - f) <= 1e-4 * max(abs(f), 1e-2 * scale_p), (i, gp[i], f)
+
+
+def test_adjoint_with_particles_leaving_the_box():
+    """Hot electrons: many leave through the absorbing faces during the run
+    (removed particles drop out of the objective and of later steps)."""
+    from pic3d_b200.adjoint import objective_and_grad
+    from pic3d_b200.simulation import Simulation
+    from pic3d_b200.workloads import PARTICLE_DTYPE
+    spec = small_spec("fp64", u_th=0.4, steps=20)
+    knots, prof = params(spec)
+    recs = spec.base_particles()
+    recs["weight"] = spec.weights(recs["x"], knots)
+    with Simulation(spec.workload, precision="fp64") as sim:   # compacting run: count the survivors
+        sim.upload_particles(0, recs)
+        sim.upload_particles(1, np.zeros(0, PARTICLE_DTYPE))
+        sim.initial_push()
+        sim.run_main_time_loop(spec.workload.steps)
+        left = len(recs) - sim.num_particles(0)
+    assert left > len(recs) // 20, left
+    _, gk, gp, _ = objective_and_grad(spec, knots, prof)
+    for i in range(spec.n_knots):
+        f = fd(spec, knots, prof, "knot", i, 1e-6)
+        assert abs(gk[i] - f) <= 1e-4 * max(abs(f), 1e-3 * np.abs(gk).max()), (i, gk[i], f)
+    for i in [5, 6]:
+        f = fd(spec, knots, prof, "prof", i, 1e-5)
+        assert abs(gp[i] - f) <= 1e-4 * max(abs(f), 1e-2 * np.abs(gp).max()), (i, gp[i], f)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_smooth_window_seeds_positions(precision):
+    """With ramps the objective depends on the final positions: the position
+    adjoint seeded by the window's slope must match finite differences."""
+    import dataclasses
+
+    from pic3d_b200.adjoint import objective_and_grad
+    spec = dataclasses.replace(small_spec("fp64", mem=4), window=(4.0, 20.0), ramp=5.0)
+    knots, prof = params(spec)
+    _, gk, gp, _ = objective_and_grad(spec, knots, prof)
+    hard = objective_and_grad(dataclasses.replace(spec, ramp=0.0), knots, prof)
+    assert np.linalg.norm(gk - hard[1]) > 1e-3 * np.linalg.norm(gk), "the ramps must change the gradient"
+    for i in range(spec.n_knots):
+        f = fd(spec, knots, prof, "knot", i, 1e-5)
+        assert abs(gk[i] - f) <= 1e-4 * max(abs(f), 1e-3 * np.abs(gk).max()), (i, gk[i], f)
+    for i in [5, 10]:
+        f = fd(spec, knots, prof, "prof", i, 1e-4)
+        assert abs(gp[i] - f) <= 1e-4 * max(abs(f), 1e-2 * np.abs(gp).max()), (i, gp[i], f)
+    if precision == "fp32":
+        s32 = dataclasses.replace(spec, precision="fp32")
+        _, k32, p32, _ = objective_and_grad(s32, knots, prof)
+        assert np.linalg.norm(k32 - gk) <= 1e-4 * np.linalg.norm(gk)
+        assert np.linalg.norm(p32 - gp) <= 1e-3 * np.linalg.norm(gp)
 
 
 def test_segments_do_not_change_the_gradient():
