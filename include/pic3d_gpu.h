@@ -138,6 +138,44 @@ int pic_run_steps(pic_ctx *ctx, int nsteps);
 int pic_get_step(const pic_ctx *ctx, int *step);
 int pic_set_step(pic_ctx *ctx, int step);
 
+/* ---- the rest of the reference's per-step call surface ---------------- */
+/* update_electromagnetic_fields (src/field.cpp:24-54): both curls with the
+ * full dt, E then B, each followed by its halo (unused by the reference's
+ * own loop) */
+int pic_update_fields_full(pic_ctx *ctx);
+/* exchange_boundary_data(data) (src/mpi_utils.cpp:9-60) on one field array
+ * (PIC_EX..PIC_BZ): the periodic ghost fill */
+int pic_exchange_boundary(pic_ctx *ctx, int array);
+/* exchange_boundary_current_fixed(data) (src/mpi_utils.cpp:232-417) on one
+ * ring array (PIC_JX..PIC_RHO1): the periodic fold */
+int pic_exchange_current(pic_ctx *ctx, int array);
+/* filter_field(data) (src/particle.cpp:520-567) on one ring array: one
+ * binomial (1/4, 1/2, 1/4) pass along x, then y, then z over the physical
+ * points */
+int pic_filter_current(pic_ctx *ctx, int array);
+/* binomial_filter_currents() (src/particle.cpp:569-574): jx, jy, jz */
+int pic_binomial_filter_currents(pic_ctx *ctx);
+/* currents_particle(p, kind) (src/particle.cpp:372-515) for one 144-byte
+ * record: its move from (x_old, y_old, z_old) to (x, y, z) deposited into J
+ * and rho_particle[kind]; a move of more than one cell is PIC_EOOB */
+int pic_deposit_particle(pic_ctx *ctx, int kind, const void *record);
+/* Device evaluation of the reference's scalar helpers with the kernels' own
+ * code:
+ *   PIC_EVAL_SHAPE2       shape_function_2(x)       in[1]  out[3]  (src/particle.cpp:8-19)
+ *   PIC_EVAL_SHAPE4       shape_function_4(x)       in[1]  out[5]  (src/particle.cpp:21-48)
+ *   PIC_EVAL_G_FACTOR     g_factor(x)               in[1]  out[1]  (src/particle.cpp:603-637;
+ *                         outside the table: PIC_ERANGE)
+ *   PIC_EVAL_LASER_PULSE  generate_laser_pulse(t,x) in[2]  out[1]  (src/boundary.cpp:8-27)
+ *   PIC_EVAL_GPULSE       Gpulse(t,x,y,z)           in[4]  out[1]  (src/boundary.cpp:29-40) */
+enum {
+    PIC_EVAL_SHAPE2 = 0,
+    PIC_EVAL_SHAPE4 = 1,
+    PIC_EVAL_G_FACTOR = 2,
+    PIC_EVAL_LASER_PULSE = 3,
+    PIC_EVAL_GPULSE = 4
+};
+int pic_eval(pic_ctx *ctx, int what, const double *in, int nin, double *out, int nout);
+
 /* Wait for the context's stream and report any device-side status. */
 int pic_synchronize(pic_ctx *ctx);
 /* The context's cudaStream_t (as void*), for callers that time or order work. */

@@ -55,7 +55,12 @@ EXPORTS = [
     "pic_profile_reset", "pic_save", "pic_load", "pic_field_diagnostics_noalloc", "pic_checkpoint_save",
     "pic_checkpoint_restore", "pic_adjoint_tape", "pic_adjoint_record", "pic_adjoint_seed_kinetic",
     "pic_adjoint_backward", "pic_adjoint_weight_grad", "pic_adjoint_profile_grad", "pic_adjoint_release",
+    "pic_update_fields_full", "pic_exchange_boundary", "pic_exchange_current", "pic_filter_current",
+    "pic_binomial_filter_currents", "pic_deposit_particle", "pic_eval",
 ]
+
+# pic_eval selectors (include/pic3d_gpu.h)
+EVAL_SHAPE2, EVAL_SHAPE4, EVAL_G_FACTOR, EVAL_LASER_PULSE, EVAL_GPULSE = range(5)
 
 
 def load(path: str = LIB_PATH):
@@ -83,7 +88,8 @@ def load(path: str = LIB_PATH):
     lib.pic_set_laser_profile.argtypes = [V, V, ctypes.c_int]
     lib.pic_radiating_boundary.argtypes = [V, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     for n in ["pic_update_fields_first", "pic_update_fields_second", "pic_clear_currents", "pic_exchange_currents",
-              "pic_initial_push", "pic_synchronize", "pic_profile_reset"]:
+              "pic_initial_push", "pic_synchronize", "pic_profile_reset", "pic_update_fields_full",
+              "pic_binomial_filter_currents"]:
         getattr(lib, n).argtypes = [V]
     lib.pic_update_particles.argtypes = [V, ctypes.c_int]
     lib.pic_exchange_particles.argtypes = [V, ctypes.c_int]
@@ -104,6 +110,11 @@ def load(path: str = LIB_PATH):
     lib.pic_adjoint_weight_grad.argtypes = [V, ctypes.c_int, V, _I64]
     lib.pic_adjoint_profile_grad.argtypes = [V, V, ctypes.c_int]
     lib.pic_adjoint_release.argtypes = [V]
+    lib.pic_exchange_boundary.argtypes = [V, ctypes.c_int]
+    lib.pic_exchange_current.argtypes = [V, ctypes.c_int]
+    lib.pic_filter_current.argtypes = [V, ctypes.c_int]
+    lib.pic_deposit_particle.argtypes = [V, ctypes.c_int, V]
+    lib.pic_eval.argtypes = [V, ctypes.c_int, P(_D), ctypes.c_int, P(_D), ctypes.c_int]
     lib.pic_save.argtypes = [V, ctypes.c_char_p]
     lib.pic_load.argtypes = [V, ctypes.c_char_p]
     _lib = lib

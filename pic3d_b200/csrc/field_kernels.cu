@@ -10,6 +10,7 @@
 // broadcasts its images; each point has exactly one owning thread, so no
 // atomics are needed.
 #include "pic_kernels.cuh"
+#include "push_core.cuh"
 
 namespace pic {
 
@@ -334,67 +335,114 @@ __global__ void radiating_boundary_kernel(Geom g, LaserArgs L, const real *__res
 // host launchers
 
 template <typename real>
-static void fields_e(pic_ctx *c) {
+static void fields_e(pic_ctx *c, double coef) {
     const Geom &g = c->g;
     dim3 blk(32, 8), grd((g.n[0] + 31) / 32, (g.n[1] + 7) / 8, g.n[2]);
     real **F = (real **)c->field;
     real **R = (real **)c->ring;
     update_e_kernel<real><<<grd, blk, 0, c->stream>>>(g, F[0], F[1], F[2], F[3], F[4], F[5], R[0], R[1], R[2],
-                                                      (real)c->p.dt_half, (real)(1.0 / c->p.dx),
+                                                      (real)coef, (real)(1.0 / c->p.dx),
                                                       (real)(1.0 / c->p.dy), (real)(1.0 / c->p.dz));
 }
 
 template <typename real>
-static void fields_b(pic_ctx *c) {
+static void fields_b(pic_ctx *c, double coef) {
     const Geom &g = c->g;
     dim3 blk(32, 8), grd((g.n[0] + 31) / 32, (g.n[1] + 7) / 8, g.n[2]);
     real **F = (real **)c->field;
-    update_b_kernel<real><<<grd, blk, 0, c->stream>>>(g, F[0], F[1], F[2], F[3], F[4], F[5], (real)c->p.dt_half,
+    update_b_kernel<real><<<grd, blk, 0, c->stream>>>(g, F[0], F[1], F[2], F[3], F[4], F[5], (real)coef,
                                                       (real)(1.0 / c->p.dx), (real)(1.0 / c->p.dy),
                                                       (real)(1.0 / c->p.dz));
 }
 
+// ghost fill of up to three field arrays (null entries skipped)
 template <typename real>
-static void ghost_fill3(pic_ctx *c, int first) {
+static void ghost_fill(pic_ctx *c, void *a0, void *a1, void *a2) {
     ShellPlan pl = ghost_plan(c->g);
     long long n = pl.start[pl.ns];
     if (n == 0) return;
-    real **F = (real **)c->field;
-    ghost_fill_kernel<real><<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->g, pl, F[first], F[first + 1],
-                                                                               F[first + 2]);
+    ghost_fill_kernel<real><<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->g, pl, (real *)a0, (real *)a1,
+                                                                               (real *)a2);
 }
 
-void launch_update_e(pic_ctx *c) {
+static void ghost_fill_any(pic_ctx *c, void *a0, void *a1, void *a2) {
+    if (c->fp32) ghost_fill<float>(c, a0, a1, a2); else ghost_fill<double>(c, a0, a1, a2);
+}
+
+void launch_update_e(pic_ctx *c, double coef) {
     prof_begin(c, "yee_update_e");
-    if (c->fp32) fields_e<float>(c); else fields_e<double>(c);
+    if (c->fp32) fields_e<float>(c, coef); else fields_e<double>(c, coef);
     prof_end(c);
     prof_begin(c, "ghost_fill");
-    if (c->fp32) ghost_fill3<float>(c, 0); else ghost_fill3<double>(c, 0);
+    ghost_fill_any(c, c->field[0], c->field[1], c->field[2]);
     prof_end(c);
 }
 
-void launch_update_b(pic_ctx *c) {
+void launch_update_b(pic_ctx *c, double coef) {
     prof_begin(c, "yee_update_b");
-    if (c->fp32) fields_b<float>(c); else fields_b<double>(c);
+    if (c->fp32) fields_b<float>(c, coef); else fields_b<double>(c, coef);
     prof_end(c);
     prof_begin(c, "ghost_fill");
-    if (c->fp32) ghost_fill3<float>(c, 3); else ghost_fill3<double>(c, 3);
+    ghost_fill_any(c, c->field[3], c->field[4], c->field[5]);
     prof_end(c);
 }
 
+void launch_ghost_fill_one(pic_ctx *c, int array) {
+    prof_begin(c, "ghost_fill");
+    ghost_fill_any(c, c->field[array], nullptr, nullptr);
+    prof_end(c);
+}
+
+// fold of the ring arrays selected by `mask` (bit k: jx, jy, jz, rho0, rho1)
 template <typename real>
-static void fold(pic_ctx *c) {
+static void fold(pic_ctx *c, unsigned mask) {
     ShellPlan pl = fold_plan(c->g);
     long long n = pl.start[pl.ns];
     if (n == 0) return;
-    real **R = (real **)c->ring;
+    real *R[5];
+    for (int k = 0; k < 5; ++k) R[k] = (mask >> k & 1u) ? (real *)c->ring[k] : nullptr;
     dim3 grd((unsigned)((n + 255) / 256), 5);
     fold_kernel<real><<<grd, 256, 0, c->stream>>>(c->g, pl, R[0], R[1], R[2], R[3], R[4]);
 }
 
-void launch_fold_currents(pic_ctx *c) {
+void launch_fold_currents(pic_ctx *c, unsigned mask) {
     prof_begin(c, "current_fold");
-    if (c->fp32) fold<float>(c); else fold<double>(c);
+    if (c->fp32) fold<float>(c, mask); else fold<double>(c, mask);
+    prof_end(c);
+}
+
+// ---------------------------------------------------------------------------
+// One pass of the binomial current filter (filter_field,
+// src/particle.cpp:520-567) along `axis`: every physical point becomes
+// 0.25 a[i-1] + 0.5 a[i] + 0.25 a[i+1] of the values before the pass (`src`
+// is a copy of the array taken before it); all other points are untouched.
+// The products by 1/4 and 1/2 are exact, so the sum is the reference's
+// (0.25 a + 0.5 b) + 0.25 c rounded twice, contracted or not.
+template <typename real>
+__global__ void binomial_pass_kernel(Geom g, int axis, const real *__restrict__ src, real *__restrict__ dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    const int k = blockIdx.z;
+    if (i >= g.n[0]) return;
+    const int fx = i + g.mem, fy = j + g.mem, fz = k + g.mem;
+    const long long at = g.ri(fz, fy, fx);
+    const long long step = axis == 0 ? 1 : (axis == 1 ? (long long)g.r[0] : (long long)g.rxy);
+    const real a = src[at - step], b = src[at], cc = src[at + step];
+    dst[at] = (real(0.25) * a + real(0.5) * b) + real(0.25) * cc;
+}
+
+void launch_binomial_pass(pic_ctx *c, int ring_index, int axis, void *scratch) {
+    const Geom &g = c->g;
+    const size_t bytes = (size_t)g.rsz * (c->fp32 ? 4 : 8);
+    cudaMemcpyAsync(scratch, c->ring[ring_index], bytes, cudaMemcpyDeviceToDevice, c->stream);
+    dim3 grd((unsigned)((g.n[0] + 127) / 128), (unsigned)g.n[1], (unsigned)g.n[2]);
+    prof_begin(c, "binomial_filter");
+    if (c->fp32)
+        binomial_pass_kernel<float><<<grd, 128, 0, c->stream>>>(g, axis, (const float *)scratch,
+                                                                 (float *)c->ring[ring_index]);
+    else
+        binomial_pass_kernel<double><<<grd, 128, 0, c->stream>>>(g, axis, (const double *)scratch,
+                                                                  (double *)c->ring[ring_index]);
     prof_end(c);
 }
 
@@ -407,9 +455,8 @@ static void rb(pic_ctx *c, const LaserArgs &L) {
     radiating_boundary_kernel<real><<<grd, blk, 0, c->stream>>>(g, L, F[1], F[2], F[3], F[4], F[5], R[1], R[2]);
 }
 
-void launch_radiating_boundary(pic_ctx *c, int is_left, int is_right, int step) {
+static LaserArgs laser_args(const pic_ctx *c, double time) {
     const PicParams &p = c->p;
-    if (p.rank_period[0]) return;  // both x faces have a neighbour: nothing written
     LaserArgs L{};
     L.Pi = p.Pi; L.omega = p.omega; L.l0 = p.l0; L.Lx = p.Lx; L.dt = p.dt; L.dx = p.dx; L.dy = p.dy; L.dz = p.dz;
     L.amp = p.laser_amplitude; L.dur = p.laser_pulse_duration; L.start = p.laser_start_time;
@@ -417,11 +464,59 @@ void launch_radiating_boundary(pic_ctx *c, int is_left, int is_right, int step) 
     L.pol = p.laser_polarization; L.envelope = p.laser_envelope;
     L.profile = (p.laser_profile == 1 && c->d_profile) ? 1 : 0;
     L.profile_n = c->profile_n; L.coef = c->d_profile;
-    L.time = step * p.dt;
+    L.time = time;
+    return L;
+}
+
+void launch_radiating_boundary(pic_ctx *c, int is_left, int is_right, int step) {
+    if (c->p.rank_period[0]) return;  // both x faces have a neighbour: nothing written
+    LaserArgs L = laser_args(c, step * c->p.dt);
     L.is_left = is_left; L.is_right = is_right;
     prof_begin(c, "radiating_boundary");
     if (c->fp32) rb<float>(c, L); else rb<double>(c, L);
     prof_end(c);
+}
+
+// ---------------------------------------------------------------------------
+// Device evaluation of the reference's scalar helpers with the same device
+// code the kernels use: shape_function_2 / _4 (src/particle.cpp:8-48) at an
+// absolute buffer coordinate, g_factor (:603-637), generate_laser_pulse and
+// Gpulse (src/boundary.cpp:8-40, Gaussian transverse factor).
+__global__ void eval_kernel(Geom g, LaserArgs L, const double *tab, int tab_n, int what, double a0, double a1,
+                            double a2, double a3, double *out, unsigned *status) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    switch (what) {
+        case 0: {   // quadratic shape at x: delta from the nearest node (int)(x + 0.5)
+            double w[3];
+            shape_weights(a0 - (double)(int)(a0 + 0.5), w);
+            for (int q = 0; q < 3; ++q) out[q] = w[q];
+            break;
+        }
+        case 1: {   // quartic shape
+            double w[5];
+            shape_weights(a0 - (double)(int)(a0 + 0.5), w);
+            for (int q = 0; q < 5; ++q) out[q] = w[q];
+            break;
+        }
+        case 2:     // g factor: out of the table's range is reported through status
+            out[0] = g_factor_dev(tab, tab_n, a0, status);
+            break;
+        case 3:     // envelope (time, position)
+            out[0] = laser_envelope(L, a0, a1);
+            break;
+        case 4:     // Gpulse(time, x, y, z)
+            L.time = a0;
+            L.profile = 0;
+            out[0] = gpulse(L, g, a0, a1, a2, a3, 0, 0);
+            break;
+    }
+}
+
+int launch_eval(pic_ctx *c, int what, const double *in, double *d_out) {
+    LaserArgs L = laser_args(c, 0.0);
+    eval_kernel<<<1, 32, 0, c->stream>>>(c->g, L, c->d_gtab, c->gtab_n, what, in[0], in[1], in[2], in[3], d_out,
+                                         c->d_status);
+    return 0;
 }
 
 }  // namespace pic

@@ -425,4 +425,52 @@ void launch_convert_array(pic_ctx *c, void *dst, const void *src, long long n, i
     else convert_kernel<<<b, 256, 0, c->stream>>>((float *)src, (double *)dst, n, 0);
 }
 
+// ---------------------------------------------------------------------------
+// Deposit of one particle's move from (xo, yo, zo) to (xn, yn, zn), absolute
+// cell coordinates, with charge x weight qw: the reference's
+// currents_particle (src/particle.cpp:372-515) for a single record, through
+// the same deposit code as the push kernels (J always, rho when enabled).
+template <typename real, int P>
+__global__ void deposit_one_kernel(PushArgs<real> a, double xo, double yo, double zo, double xn, double yn,
+                                   double zn, double qw) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    constexpr int H = P / 2;
+    const Geom &g = a.g;
+    const double po[3] = {xo, yo, zo}, pn[3] = {xn, yn, zn};
+    int i1[3], i2[3];
+    double d0[3], d1[3];
+    for (int d = 0; d < 3; ++d) {
+        const double x1 = po[d] - (double)(1 - g.mem), x2 = pn[d] - (double)(1 - g.mem);
+        if (!(x1 >= 0.0 && x2 >= 0.0 && x1 < (double)g.f[d] && x2 < (double)g.f[d])) {
+            set_status(a.status, ST_OOB);
+            return;
+        }
+        i1[d] = (int)(x1 + 0.5);
+        i2[d] = (int)(x2 + 0.5);
+        d0[d] = x1 - (double)i1[d];
+        d1[d] = x2 - (double)i2[d];
+        // the deposit span [min - H, max + H + 1) must lie in the ring (-1 .. f)
+        if (abs(i2[d] - i1[d]) > 1 || min(i1[d], i2[d]) - H < -1 || max(i1[d], i2[d]) + H + 1 > g.f[d]) {
+            set_status(a.status, abs(i2[d] - i1[d]) > 1 ? ST_CFL : ST_OOB);
+            return;
+        }
+    }
+    View<const real> fv[6];
+    GlobalAcc<real> acc;
+    global_views(a, fv, acc);
+    deposit<real, P>(acc, a.d_dt, i1, d0, i2, d1, (real)qw);
+}
+
+void launch_deposit_one(pic_ctx *c, int kind, const double (&xo)[3], const double (&xn)[3], double qw) {
+    if (c->fp32) {
+        PushArgs<float> a = make_push_args<float>(c, kind);
+        if (c->order == 2) deposit_one_kernel<float, 3><<<1, 32, 0, c->stream>>>(a, xo[0], xo[1], xo[2], xn[0], xn[1], xn[2], qw);
+        else deposit_one_kernel<float, 5><<<1, 32, 0, c->stream>>>(a, xo[0], xo[1], xo[2], xn[0], xn[1], xn[2], qw);
+    } else {
+        PushArgs<double> a = make_push_args<double>(c, kind);
+        if (c->order == 2) deposit_one_kernel<double, 3><<<1, 32, 0, c->stream>>>(a, xo[0], xo[1], xo[2], xn[0], xn[1], xn[2], qw);
+        else deposit_one_kernel<double, 5><<<1, 32, 0, c->stream>>>(a, xo[0], xo[1], xo[2], xn[0], xn[1], xn[2], qw);
+    }
+}
+
 }  // namespace pic

@@ -532,15 +532,15 @@ int pic_radiating_boundary(pic_ctx *c, int is_left, int is_right, int step) {
 
 int pic_update_fields_first(pic_ctx *c) {
     if (!c) return PIC_EINVAL;
-    launch_update_e(c);
-    launch_update_b(c);
+    launch_update_e(c, c->p.dt_half);
+    launch_update_b(c, c->p.dt_half);
     return launch_check(c, "update_fields_first");
 }
 
 int pic_update_fields_second(pic_ctx *c) {
     if (!c) return PIC_EINVAL;
-    launch_update_b(c);
-    launch_update_e(c);
+    launch_update_b(c, c->p.dt_half);
+    launch_update_e(c, c->p.dt_half);
     return launch_check(c, "update_fields_second");
 }
 
@@ -583,6 +583,71 @@ int pic_exchange_currents(pic_ctx *c) {
     if (!c) return PIC_EINVAL;
     launch_fold_currents(c);
     return launch_check(c, "exchange_currents");
+}
+
+int pic_update_fields_full(pic_ctx *c) {
+    if (!c) return PIC_EINVAL;
+    launch_update_e(c, c->p.dt);
+    launch_update_b(c, c->p.dt);
+    return launch_check(c, "update_fields_full");
+}
+
+int pic_exchange_boundary(pic_ctx *c, int array) {
+    if (!c) return PIC_EINVAL;
+    if (array < PIC_EX || array > PIC_BZ) return fail(c, PIC_EINVAL, "exchange_boundary: not a field array");
+    launch_ghost_fill_one(c, array);
+    return launch_check(c, "exchange_boundary");
+}
+
+int pic_exchange_current(pic_ctx *c, int array) {
+    if (!c) return PIC_EINVAL;
+    if (array < PIC_JX || array > PIC_RHO1) return fail(c, PIC_EINVAL, "exchange_current: not a ring array");
+    launch_fold_currents(c, 1u << (array - PIC_JX));
+    return launch_check(c, "exchange_current");
+}
+
+int pic_filter_current(pic_ctx *c, int array) {
+    if (!c) return PIC_EINVAL;
+    if (array < PIC_JX || array > PIC_RHO1) return fail(c, PIC_EINVAL, "filter_current: not a ring array");
+    int r = ensure_stage(c, (size_t)c->g.rsz * real_size(c));
+    if (r) return r;
+    for (int axis = 0; axis < 3; ++axis) launch_binomial_pass(c, array - PIC_JX, axis, c->d_stage);
+    return launch_check(c, "filter_current");
+}
+
+int pic_binomial_filter_currents(pic_ctx *c) {
+    int r = PIC_OK;
+    for (int a = PIC_JX; a <= PIC_JZ && r == PIC_OK; ++a) r = pic_filter_current(c, a);
+    return r;
+}
+
+int pic_deposit_particle(pic_ctx *c, int kind, const void *record) {
+    if (!c || kind < 0 || kind > 1 || !record) return PIC_EINVAL;
+    // 144-byte reference record: x, y, z at bytes 8..31, x_old.. at 32..55,
+    // charge at 112, weight at 128
+    const unsigned char *b = (const unsigned char *)record;
+    double xn[3], xo[3], q, w;
+    std::memcpy(xn, b + 8, sizeof xn);
+    std::memcpy(xo, b + 32, sizeof xo);
+    std::memcpy(&q, b + 112, sizeof q);
+    std::memcpy(&w, b + 128, sizeof w);
+    launch_deposit_one(c, kind, xo, xn, q * w);
+    int r = launch_check(c, "deposit_particle");
+    return r ? r : sync_status(c);
+}
+
+int pic_eval(pic_ctx *c, int what, const double *in, int nin, double *out, int nout) {
+    static const int need_in[] = {1, 1, 1, 2, 4}, need_out[] = {3, 5, 1, 1, 1};
+    if (!c || what < 0 || what > 4 || !in || !out) return PIC_EINVAL;
+    if (nin < need_in[what] || nout < need_out[what]) return fail(c, PIC_EINVAL, "pic_eval: argument count");
+    if (what == PIC_EVAL_G_FACTOR && !c->d_gtab) return fail(c, PIC_EINVAL, "pic_eval: no g table loaded");
+    double a[4] = {0, 0, 0, 0};
+    for (int i = 0; i < need_in[what]; ++i) a[i] = in[i];
+    launch_eval(c, what, a, c->d_diag);
+    int r = launch_check(c, "eval");
+    if (r) return r;
+    CK(cudaMemcpyAsync(out, c->d_diag, (size_t)need_out[what] * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    return sync_status(c);
 }
 
 int pic_initial_push(pic_ctx *c) {

@@ -10,10 +10,13 @@ void prof_begin(pic_ctx *c, const char *name);
 void prof_end(pic_ctx *c);
 
 // field_kernels.cu
-void launch_update_e(pic_ctx *c);
-void launch_update_b(pic_ctx *c);
-void launch_fold_currents(pic_ctx *c);
+void launch_update_e(pic_ctx *c, double coef);   // E += coef (curl B - J), then the E ghost fill
+void launch_update_b(pic_ctx *c, double coef);   // B -= coef curl E, then the B ghost fill
+void launch_ghost_fill_one(pic_ctx *c, int array);
+void launch_fold_currents(pic_ctx *c, unsigned mask = 31u);
 void launch_radiating_boundary(pic_ctx *c, int is_left, int is_right, int step);
+void launch_binomial_pass(pic_ctx *c, int ring_index, int axis, void *scratch);
+int launch_eval(pic_ctx *c, int what, const double *in, double *d_out);
 
 // particle_kernels.cu
 void launch_push(pic_ctx *c, int kind);
@@ -22,6 +25,7 @@ void launch_remove(pic_ctx *c, int kind);
 void launch_upload_particles(pic_ctx *c, int kind, const void *d_records, int64_t n, int64_t offset);
 void launch_download_particles(pic_ctx *c, int kind, void *d_records, int64_t n, int64_t offset);
 void launch_convert_array(pic_ctx *c, void *dst, const void *src, long long n, int to_device);
+void launch_deposit_one(pic_ctx *c, int kind, const double (&xo)[3], const double (&xn)[3], double qw);
 
 // tile_kernels.cu
 void launch_sort(pic_ctx *c, int kind);
