@@ -220,8 +220,8 @@ __device__ __forceinline__ void span_pair(int i1, const T (&a0)[P], int i2, cons
 // ds = s1 - s0, axes `u` and `v` the weight
 // W = 1/3 s0u s0v + 1/6 s1u s0v + 1/6 s0u s1v + 1/3 s1u s1v.
 // Returns G1 = sum(lam * J) / w and adds dG1/ds0, dG1/ds1 into g0, g1.
-template <int P>
-__device__ __forceinline__ double esirkepov_adj(const double *lam, int sc, int su, int sv, int lc, int lu, int lv,
+template <int P, typename LT>
+__device__ __forceinline__ double esirkepov_adj(const LT *lam, int sc, int su, int sv, int lc, int lu, int lv,
                                                 double coef, const double (&s0c)[P + 1], const double (&s1c)[P + 1],
                                                 const double (&s0u)[P + 1], const double (&s1u)[P + 1],
                                                 const double (&s0v)[P + 1], const double (&s1v)[P + 1],
@@ -247,11 +247,11 @@ __device__ __forceinline__ double esirkepov_adj(const double *lam, int sc, int s
             if (a >= lu) break;
             const double W = third * s0u[a] * s0b + sixth * s1u[a] * s0b + sixth * s0u[a] * s1b + third * s1u[a] * s1b;
             double T = 0.0;
-            const double *row = lam + b * sv + a * su;
+            const LT *row = lam + b * sv + a * su;
 #pragma unroll
             for (int q = 0; q < P; ++q) {
                 if (q >= lc - 1) break;
-                const double l = row[q * sc];
+                const double l = (double)__ldg(row + q * sc);
                 T += C[q] * l;
                 M[q] += l * W;
             }
@@ -352,6 +352,9 @@ __global__ void __launch_bounds__(128) adj_push_kernel(AdjPushArgs<real> a) {
             set_status(a.status, ST_OOB);
             continue;
         }
+        // ---- gather with gradients (Yee staggering, particle.cpp:207-259) -
+        real ev[6], eg[6][3];
+        {
         real wp[3][P], wd[3][P], gp[3][P], gd[3][P];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
@@ -360,44 +363,29 @@ __global__ void __launch_bounds__(128) adj_push_kernel(AdjPushArgs<real> a) {
             shape_derivs(dp[d], gp[d]);
             shape_derivs(dd[d], gd[d]);
         }
-        // ---- gather with gradients (Yee staggering, particle.cpp:207-259) -
-        real ev[6], eg[6][3];
         gather_grad<real, P>(a.f[0], g, id[0] - H, ip[1] - H, ip[2] - H, wd[0], wp[1], wp[2], gd[0], gp[1], gp[2], ev[0], eg[0]);
         gather_grad<real, P>(a.f[1], g, ip[0] - H, id[1] - H, ip[2] - H, wp[0], wd[1], wp[2], gp[0], gd[1], gp[2], ev[1], eg[1]);
         gather_grad<real, P>(a.f[2], g, ip[0] - H, ip[1] - H, id[2] - H, wp[0], wp[1], wd[2], gp[0], gp[1], gd[2], ev[2], eg[2]);
         gather_grad<real, P>(a.f[3], g, ip[0] - H, id[1] - H, id[2] - H, wp[0], wd[1], wd[2], gp[0], gd[1], gd[2], ev[3], eg[3]);
         gather_grad<real, P>(a.f[4], g, id[0] - H, ip[1] - H, id[2] - H, wd[0], wp[1], wd[2], gd[0], gp[1], gd[2], ev[4], eg[4]);
         gather_grad<real, P>(a.f[5], g, id[0] - H, id[1] - H, ip[2] - H, wd[0], wd[1], wp[2], gd[0], gd[1], gp[2], ev[5], eg[5]);
+        }
         // ---- Boris Jacobian: three passes of three tangents (p, e, b) -----
         const real pin[3] = {a.px[p], a.py[p], a.pz[p]};
-        real jac[6][9];   // d(p', disp) / d(p, e, b)
-        real pn_v[3], disp_v[3];
-#pragma unroll
-        for (int pass = 0; pass < 3; ++pass) {
-            Dual<real, 3> P_[3], E_[3], B_[3], pn[3], ds[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                P_[d] = dconst<real, 3>(pin[d]);
-                E_[d] = dconst<real, 3>(ev[d]);
-                B_[d] = dconst<real, 3>(ev[3 + d]);
-            }
+        // values only here (the displacement fixes the new position); the
+        // tangents are formed after the deposit adjoint, contracted at once
+        real disp_v[3];
+        {
+            Dual<real, 1> P_[3], E_[3], B_[3], pn[3], ds[3];
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                if (pass == 0) P_[d].d[d] = real(1);
-                if (pass == 1) E_[d].d[d] = real(1);
-                if (pass == 2) B_[d].d[d] = real(1);
+                P_[d] = dconst<real, 1>(pin[d]);
+                E_[d] = dconst<real, 1>(ev[d]);
+                B_[d] = dconst<real, 1>(ev[3 + d]);
             }
-            boris_dual<real, 3>(P_, E_, B_, a.qm, a.dt_d, pn, ds);
+            boris_dual<real, 1>(P_, E_, B_, a.qm, a.dt_d, pn, ds);
 #pragma unroll
-            for (int o = 0; o < 3; ++o) {
-#pragma unroll
-                for (int t = 0; t < 3; ++t) {
-                    jac[o][3 * pass + t] = pn[o].d[t];
-                    jac[3 + o][3 * pass + t] = ds[o].d[t];
-                }
-                pn_v[o] = pn[o].v;
-                disp_v[o] = ds[o].v;
-            }
+            for (int o = 0; o < 3; ++o) disp_v[o] = ds[o].v;
         }
         // ---- new position, as the forward deposit forms it ----------------
         int i2[3];
@@ -426,18 +414,15 @@ __global__ void __launch_bounds__(128) adj_push_kernel(AdjPushArgs<real> a) {
             continue;
         }
         // ---- deposit adjoint ----------------------------------------------
-        double s0[3][P + 1], s1[3][P + 1], t0[3][P + 1], t1[3][P + 1];   // weights and their derivatives
-        double g0[3][P + 1], g1[3][P + 1];                                // dG1 / d(weights)
+        double s0[3][P + 1], s1[3][P + 1];   // weights on the common span
+        double g0[3][P + 1], g1[3][P + 1];   // dG1 / d(weights)
         int base[3], len[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            double w0[P], w1[P], v0[P], v1[P];
+            double w0[P], w1[P];
             shape_weights(d0[d], w0);
             shape_weights(d2[d], w1);
-            shape_derivs(d0[d], v0);
-            shape_derivs(d2[d], v1);
             span_pair<double, P>(ip[d], w0, i2[d], w1, s0[d], s1[d]);
-            span_pair<double, P>(ip[d], v0, i2[d], v1, t0[d], t1[d]);
             base[d] = min(ip[d], i2[d]) - H;
             len[d] = P + abs(i2[d] - ip[d]);
 #pragma unroll
@@ -445,17 +430,12 @@ __global__ void __launch_bounds__(128) adj_push_kernel(AdjPushArgs<real> a) {
         }
         const double qd = (double)a.charge;
         double G1 = 0.0;
-        double lbuf[(P + 1) * (P + 1) * (P + 1)];
-        // Jx: running sum along x, weight from y and z (particle.cpp:427-450)
+        // Jx: running sum along x, weight from y and z (particle.cpp:427-450);
+        // the J adjoints are read in place from the ring buffers
 #pragma unroll 1
         for (int comp = 0; comp < 3; ++comp) {
-            const real *lj = a.lj[comp];
-            for (int k = 0; k < len[2]; ++k)
-                for (int j = 0; j < len[1]; ++j)
-                    for (int i = 0; i < len[0]; ++i)
-                        lbuf[(k * (P + 1) + j) * (P + 1) + i] =
-                            (double)__ldg(lj + g.ri(base[2] + k, base[1] + j, base[0] + i));
-            const int sX = 1, sY = P + 1, sZ = (P + 1) * (P + 1);
+            const real *lbuf = a.lj[comp] + g.ri(base[2], base[1], base[0]);
+            const int sX = 1, sY = g.r[0], sZ = g.rxy;
             if (comp == 0)
                 G1 += esirkepov_adj<P>(lbuf, sX, sY, sZ, len[0], len[1], len[2], -qd * a.d_dt[0], s0[0], s1[0],
                                        s0[1], s1[1], s0[2], s1[2], g0[0], g1[0], g0[1], g1[1], g0[2], g1[2]);
@@ -471,25 +451,47 @@ __global__ void __launch_bounds__(128) adj_push_kernel(AdjPushArgs<real> a) {
         double dGx0[3], dGx1[3];   // d G / d x_old, d G / d x_new
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
+            double v0[P], v1[P], t0[P + 1], t1[P + 1];   // weight derivatives on the span
+            shape_derivs(d0[d], v0);
+            shape_derivs(d2[d], v1);
+            span_pair<double, P>(ip[d], v0, i2[d], v1, t0, t1);
             double s_0 = 0.0, s_1 = 0.0;
 #pragma unroll
             for (int q = 0; q <= P; ++q) {
-                s_0 += g0[d][q] * t0[d][q];
-                s_1 += g1[d][q] * t1[d][q];
+                s_0 += g0[d][q] * t0[q];
+                s_1 += g1[d][q] * t1[q];
             }
             dGx0[d] = wgt * s_0;
             dGx1[d] = wgt * s_1;
         }
-        // ---- chain rule ---------------------------------------------------
+        // ---- chain rule: lin = J^T (lp', lx') with J = d(p', disp) / d(p, e,
+        // b), one forward-mode pass of three tangents per input group ------
         const real lxn[3] = {a.lx[p] + (real)dGx1[0], a.ly[p] + (real)dGx1[1], a.lz[p] + (real)dGx1[2]};
         const real lpn[3] = {a.lpx[p], a.lpy[p], a.lpz[p]};
         real lin[9];
 #pragma unroll
-        for (int t = 0; t < 9; ++t) {
-            real s = 0;
+        for (int pass = 0; pass < 3; ++pass) {
+            Dual<real, 3> P_[3], E_[3], B_[3], pn[3], ds[3];
 #pragma unroll
-            for (int o = 0; o < 3; ++o) s += lpn[o] * jac[o][t] + lxn[o] * jac[3 + o][t];
-            lin[t] = s;
+            for (int d = 0; d < 3; ++d) {
+                P_[d] = dconst<real, 3>(pin[d]);
+                E_[d] = dconst<real, 3>(ev[d]);
+                B_[d] = dconst<real, 3>(ev[3 + d]);
+            }
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                if (pass == 0) P_[d].d[d] = real(1);
+                if (pass == 1) E_[d].d[d] = real(1);
+                if (pass == 2) B_[d].d[d] = real(1);
+            }
+            boris_dual<real, 3>(P_, E_, B_, a.qm, a.dt_d, pn, ds);
+#pragma unroll
+            for (int t = 0; t < 3; ++t) {
+                real s = 0;
+#pragma unroll
+                for (int o = 0; o < 3; ++o) s += lpn[o] * pn[o].d[t] + lxn[o] * ds[o].d[t];
+                lin[3 * pass + t] = s;
+            }
         }
         real lxo[3];
 #pragma unroll
@@ -506,6 +508,12 @@ __global__ void __launch_bounds__(128) adj_push_kernel(AdjPushArgs<real> a) {
         a.lpy[p] = lin[1];
         a.lpz[p] = lin[2];
         if (a.scatter_fields) {
+            real wp[3][P], wd[3][P];   // the gather weights again (cheaper than keeping them live)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                shape_weights(dp[d], wp[d]);
+                shape_weights(dd[d], wd[d]);
+            }
             scatter_adj<real, P>(a.lf[0], g, id[0] - H, ip[1] - H, ip[2] - H, wd[0], wp[1], wp[2], lin[3]);
             scatter_adj<real, P>(a.lf[1], g, ip[0] - H, id[1] - H, ip[2] - H, wp[0], wd[1], wp[2], lin[4]);
             scatter_adj<real, P>(a.lf[2], g, ip[0] - H, ip[1] - H, id[2] - H, wp[0], wp[1], wd[2], lin[5]);
@@ -816,7 +824,9 @@ void adjoint_record_hook(pic_ctx *c) {
     std::vector<std::pair<void *, size_t>> parts;
     particle_parts(c, parts);
     for (int f = 0; f < 6; ++f) parts.push_back({c->field[f], (size_t)c->g.fsz * rsize(c)});
+    prof_begin(c, "adjoint_tape_record");
     if (blob_save(c, A->tape[A->tape_len], parts) == PIC_OK) A->tape_len++;
+    prof_end(c);
 }
 }  // namespace pic
 
@@ -888,7 +898,9 @@ static void adj_push_launch(pic_ctx *c, AdjState *A, const Blob &b, int kind, in
     a.scatter_fields = scatter;
     a.status = c->d_status;
     long long blocks = (a.n + 127) / 128;
+    prof_begin(c, "adjoint_push_deposit");
     adj_push_kernel<real, P><<<(unsigned)std::min<long long>(blocks, 148 * 16), 128, 0, c->stream>>>(a);
+    prof_end(c);
 }
 
 template <typename real>
@@ -896,18 +908,22 @@ static void adj_fields_e(pic_ctx *c, AdjState *A) {
     const Geom &g = c->g;
     real **F = (real **)A->lf;
     real **J = (real **)A->lj;
+    prof_begin(c, "adjoint_yee_e");
     adj_update_e_kernel<real><<<(unsigned)((g.fsz + 255) / 256), 256, 0, c->stream>>>(
         g, F[0], F[1], F[2], F[3], F[4], F[5], J[0], J[1], J[2], (real)c->p.dt_half, (real)(1.0 / c->p.dx),
         (real)(1.0 / c->p.dy), (real)(1.0 / c->p.dz));
+    prof_end(c);
 }
 
 template <typename real>
 static void adj_fields_b(pic_ctx *c, AdjState *A) {
     const Geom &g = c->g;
     real **F = (real **)A->lf;
+    prof_begin(c, "adjoint_yee_b");
     adj_update_b_kernel<real><<<(unsigned)((g.fsz + 255) / 256), 256, 0, c->stream>>>(
         g, F[0], F[1], F[2], F[3], F[4], F[5], (real)c->p.dt_half, (real)(1.0 / c->p.dx), (real)(1.0 / c->p.dy),
         (real)(1.0 / c->p.dz));
+    prof_end(c);
 }
 
 template <typename real>
@@ -925,7 +941,9 @@ static void adj_bc(pic_ctx *c, AdjState *A, int step) {
     real **F = (real **)A->lf;
     real **J = (real **)A->lj;
     dim3 blk(32, 8), grd((g.n[1] + 31) / 32, (g.n[2] + 7) / 8);
+    prof_begin(c, "adjoint_boundary");
     adj_bc_kernel<real><<<grd, blk, 0, c->stream>>>(B, F[0], F[1], F[2], F[3], F[4], F[5], J[1], J[2]);
+    prof_end(c);
 }
 
 template <typename real>
@@ -959,7 +977,9 @@ static int adj_backward_t(pic_ctx *c, AdjState *A, int nsteps) {
             else adj_push_launch<real, 5>(c, A, b, k, base[k], loop);
         }
         // clear_currents: J before the clear does not reach the deposit
+        prof_begin(c, "adjoint_clear");
         for (int f = 0; f < 3; ++f) cudaMemsetAsync(A->lj[f], 0, (size_t)c->g.rsz * rsize(c), c->stream);
+        prof_end(c);
         if (loop) {
             // first half (field.cpp:56-86): E then B forward
             adj_fields_b<real>(c, A);
