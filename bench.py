@@ -71,6 +71,8 @@ def workload(name, precision):
         return W.laser_underdense(nx=128, ny=64, nz=64, precision=precision)
     if name == "thermal_scaleup":
         return W.thermal_scaleup(precision=precision)
+    if name in ("thermal_o2_medium", "thermal_o4_medium"):
+        return W.thermal_scaleup(nx=128, ny=64, nz=64, mem=2 if "o2" in name else 4, precision=precision)
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -489,7 +491,7 @@ def main():
                 "dtype": "f64" if prec == "fp64" else "f32", "data": "synthetic",
                 "config": {"workload": w.name, "cells": [w.nx, w.ny, w.nz], "order": w.order,
                            "tile": args.tile, "sort_interval": args.sort_interval,
-                           "particles": npart, "particles_per_cell": sum(w.ppc), "boundaries": "absorbing+laser",
+                           "particles": npart, "particles_per_cell": sum(w.ppc), "boundaries": "periodic" if all(w.period) else "absorbing+laser",
                            "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (particle state "
                                                                    f"{npart * BYTES_PER_PARTICLE[prec] / 1e9:.1f} GB)"},
                 "cell_updates_per_s": ncell * world * args.steps / (ms / 1e3),

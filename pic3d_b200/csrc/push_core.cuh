@@ -129,16 +129,20 @@ __device__ __forceinline__ void atomic_add(float *p, float v) { atomicAdd(p, v);
 
 // Where deposited current goes.  Both accumulators address a 3D array
 // through buffer coordinates with strides (sy, sz) and offset o, like View.
-//   GlobalAcc: hardware atomics into the global ring buffers.
-//   FixedAcc:  a CTA's shared-memory tile, each value scaled to a 64-bit
-//              integer and split into 20-bit limbs added with native 32-bit
-//              integer atomics (NL = 2 limbs for FP32, 3 for FP64).  Integer
-//              sums do not depend on the order of the additions.
+// The deposit multiplies every value by coef(c) before add(c, ...).
+//   GlobalAcc: hardware atomics into the global ring buffers (coef 1).
+//   FixedAcc:  a CTA's shared-memory tile; values come scaled by
+//              coef(c) = scale[c], are rounded to a 64-bit integer and split
+//              into 20-bit limbs added with native 32-bit integer atomics
+//              (NL = 2 limbs for FP32, 3 for FP64).  Integer sums do not
+//              depend on the order of the additions.  (Shared-memory 64-bit
+//              integer atomics measured 2.6x slower on the whole kernel.)
 template <typename real>
 struct GlobalAcc {
     real *p[4];  // jx, jy, jz, rho (rho may be null)
     int sy, sz, o;
     __device__ __forceinline__ bool has_rho() const { return p[3] != nullptr; }
+    __device__ __forceinline__ real coef(int) const { return real(1); }
     __device__ __forceinline__ void add(int c, int idx, real v) const { atomic_add(p[c] + idx, v); }
 };
 
@@ -149,29 +153,25 @@ struct FixedAcc {
     int sy, sz, o;
     real scale[4];    // per component: |value * scale| < 2^(20*NL - 9)
     __device__ __forceinline__ bool has_rho() const { return p[3] != nullptr; }
-    // Exact round-to-nearest of the scaled value by the add-a-magic-constant
-    // method (the sum's low mantissa bits are the integer), split into
-    // signed limbs: FP64 q = l2*2^40 + l1*2^20 + l0 with l0, l1 in [0, 2^20);
-    // FP32 q = h*2^20 + l with |l| <= 2^19.  Adding zero is skipped.
-    __device__ __forceinline__ void add(int c, int idx, real v) const {
-        if (v == real(0)) return;
+    __device__ __forceinline__ real coef(int c) const { return scale[c]; }
+    // q is already scaled.  Rounded to the nearest integer and split into
+    // limbs q = l2*2^40 + l1*2^20 + l0 (FP64) or q = h*2^20 + l0 (FP32), with
+    // l0, l1 in [0, 2^20) and the top limb signed.  FP64 rounds by the
+    // add-a-magic-constant method (the sum's low mantissa bits are the
+    // integer), FP32 by a float-to-int conversion.  Zeros are skipped: a
+    // particle at rest (cold plasma) deposits no current.
+    __device__ __forceinline__ void add(int c, int idx, real q) const {
+        if (q == real(0)) return;
         unsigned *a = p[c] + idx;
-        if constexpr (NL == 3) {
-            const double q = (double)v * (double)scale[c];               // |q| < 2^51
+        if constexpr (NL == 3) {                                           // |q| < 2^51
             const long long qi = __double_as_longlong(q + 6755399441055744.0) - 0x4338000000000000LL;
             atomicAdd(a, (unsigned)(qi & 0xFFFFF));
             atomicAdd(a + lstride, (unsigned)((qi >> 20) & 0xFFFFF));
             atomicAdd(a + 2 * lstride, (unsigned)(int)(qi >> 40));
-        } else {
-            const float q = (float)v * (float)scale[c];                  // |q| < 2^31
-            const float magic = 12582912.0f;                             // 1.5 * 2^23
-            const float t = fmaf(q, 1.0f / 1048576.0f, magic);           // round(q / 2^20) + magic
-            const float h = t - magic;
-            const float lo = fmaf(-h, 1048576.0f, q);                     // exact, |lo| <= 2^19
-            const int li = __float_as_int(lo + magic) - 0x4B400000;
-            const int hi = __float_as_int(t) - 0x4B400000;
-            atomicAdd(a, (unsigned)li);
-            atomicAdd(a + lstride, (unsigned)hi);
+        } else {                                                           // |q| < 2^31
+            const int qi = __float2int_rn(q);
+            atomicAdd(a, (unsigned)qi & 0xFFFFFu);
+            atomicAdd(a + lstride, (unsigned)(qi >> 20));
         }
     }
 };
@@ -196,68 +196,78 @@ __device__ __forceinline__ void deposit(const Acc &acc, const real (&dxdt)[3], c
         for (int q = 0; q < P; ++q) w1[d][q] = (real)a1[q];
     }
     const real third = real(1.0 / 3.0), half = real(0.5);
-    const real cx = qw * dxdt[0], cy = qw * dxdt[1], cz = qw * dxdt[2];
+    const real cx = qw * dxdt[0] * acc.coef(0), cy = qw * dxdt[1] * acc.coef(1), cz = qw * dxdt[2] * acc.coef(2);
     const int rx = acc.sy, rxy = acc.sz;
     const int r0 = base[2] * rxy + base[1] * rx + base[0] + acc.o;
-    // Jx: running sum of ds along x times the yz weight
+    // a particle that did not move (every ds zero) adds no current
+    bool moved = false;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) moved = moved || i1[d] != i2[d] || d0[d] != d1[d];
+    if (moved) {
+        // Jx: running sum of ds along x times the yz weight
 #pragma unroll 1
-    for (int k = 0; k < len[2]; ++k) {
-        const real s0z = pick(s0[2], k), dsz = pick(ds[2], k);
+        for (int k = 0; k < len[2]; ++k) {
+            const real s0z = pick(s0[2], k), dsz = pick(ds[2], k);
 #pragma unroll
-        for (int j = 0; j <= P; ++j) {
-            if (j >= len[1]) break;
-            real wyz = s0[1][j] * s0z + half * ds[1][j] * s0z + half * s0[1][j] * dsz + third * ds[1][j] * dsz;
-            real a = 0;
-            const int row = r0 + k * rxy + j * rx;
+            for (int j = 0; j <= P; ++j) {
+                if (j >= len[1]) break;
+                real wyz = s0[1][j] * s0z + half * ds[1][j] * s0z + half * s0[1][j] * dsz + third * ds[1][j] * dsz;
+                const real cw = -cx * wyz;
+                real a = 0;
+                const int row = r0 + k * rxy + j * rx;
 #pragma unroll
-            for (int i = 0; i < P; ++i) {
-                if (i >= len[0] - 1) break;
-                a += ds[0][i];
-                acc.add(0, row + i, -cx * a * wyz);
+                for (int i = 0; i < P; ++i) {
+                    if (i >= len[0] - 1) break;
+                    a += ds[0][i];
+                    acc.add(0, row + i, cw * a);
+                }
             }
         }
-    }
-    // Jy
+        // Jy
 #pragma unroll 1
-    for (int k = 0; k < len[2]; ++k) {
-        const real s0z = pick(s0[2], k), dsz = pick(ds[2], k);
+        for (int k = 0; k < len[2]; ++k) {
+            const real s0z = pick(s0[2], k), dsz = pick(ds[2], k);
 #pragma unroll
-        for (int i = 0; i <= P; ++i) {
-            if (i >= len[0]) break;
-            real wxz = s0[0][i] * s0z + half * ds[0][i] * s0z + half * s0[0][i] * dsz + third * ds[0][i] * dsz;
-            real a = 0;
-            const int col = r0 + k * rxy + i;
+            for (int i = 0; i <= P; ++i) {
+                if (i >= len[0]) break;
+                real wxz = s0[0][i] * s0z + half * ds[0][i] * s0z + half * s0[0][i] * dsz + third * ds[0][i] * dsz;
+                const real cw = -cy * wxz;
+                real a = 0;
+                const int col = r0 + k * rxy + i;
 #pragma unroll
-            for (int j = 0; j < P; ++j) {
-                if (j >= len[1] - 1) break;
-                a += ds[1][j];
-                acc.add(1, col + j * rx, -cy * a * wxz);
+                for (int j = 0; j < P; ++j) {
+                    if (j >= len[1] - 1) break;
+                    a += ds[1][j];
+                    acc.add(1, col + j * rx, cw * a);
+                }
             }
         }
-    }
-    // Jz
+        // Jz
 #pragma unroll 1
-    for (int j = 0; j < len[1]; ++j) {
-        const real s0y = pick(s0[1], j), dsy = pick(ds[1], j);
+        for (int j = 0; j < len[1]; ++j) {
+            const real s0y = pick(s0[1], j), dsy = pick(ds[1], j);
 #pragma unroll
-        for (int i = 0; i <= P; ++i) {
-            if (i >= len[0]) break;
-            real wxy = s0[0][i] * s0y + half * ds[0][i] * s0y + half * s0[0][i] * dsy + third * ds[0][i] * dsy;
-            real a = 0;
-            const int col = r0 + j * rx + i;
+            for (int i = 0; i <= P; ++i) {
+                if (i >= len[0]) break;
+                real wxy = s0[0][i] * s0y + half * ds[0][i] * s0y + half * s0[0][i] * dsy + third * ds[0][i] * dsy;
+                const real cw = -cz * wxy;
+                real a = 0;
+                const int col = r0 + j * rx + i;
 #pragma unroll
-            for (int k = 0; k < P; ++k) {
-                if (k >= len[2] - 1) break;
-                a += ds[2][k];
-                acc.add(2, col + k * rxy, -cz * a * wxy);
+                for (int k = 0; k < P; ++k) {
+                    if (k >= len[2] - 1) break;
+                    a += ds[2][k];
+                    acc.add(2, col + k * rxy, cw * a);
+                }
             }
         }
     }
     if (acc.has_rho()) {
+        const real qwr = qw * acc.coef(3);
         const int rb = (i2[2] - H) * rxy + (i2[1] - H) * rx + (i2[0] - H) + acc.o;
 #pragma unroll 1
         for (int k = 0; k < P; ++k) {
-            const real wk = qw * pick(w1[2], k);
+            const real wk = qwr * pick(w1[2], k);
 #pragma unroll
             for (int j = 0; j < P; ++j) {
                 real wjk = wk * w1[1][j];

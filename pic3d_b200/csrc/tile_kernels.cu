@@ -452,7 +452,7 @@ __global__ void __launch_bounds__(256, tile_min_blocks<real>()) tile_push_kernel
         int lz = l / D2, r = l - lz * D2, ly = r / DE, lx = r - ly * DE;
         const unsigned *q = sa + c * NL * DS + lz * dsz + ly * dsy + lx;
         long long tot;
-        if constexpr (NL == 2) tot = ((long long)(int)q[DS] << 20) + (long long)(int)q[0];
+        if constexpr (NL == 2) tot = ((long long)(int)q[DS] << 20) + (long long)q[0];
         else tot = ((long long)(int)q[2 * DS] << 40) + ((long long)q[DS] << 20) + (long long)q[0];
         if (tot == 0) continue;
         int x = dO[0] + lx, y = dO[1] + ly, z = dO[2] + lz;
