@@ -40,6 +40,7 @@ extern "C" {
 #define PIC_ECUDA 6     /* a CUDA runtime error */
 #define PIC_EOVERFLOW 7 /* a particle bin or buffer overflowed */
 #define PIC_ERANGE 8    /* g_factor argument outside the table (src/particle.cpp:632-636) */
+#define PIC_ENOCONV 9   /* an iterative solve stopped at its iteration limit before its tolerance */
 
 /* ---- array identifiers for upload / download ------------------------ */
 enum {
@@ -188,6 +189,58 @@ int pic_get_stream(const pic_ctx *ctx, void **stream);
  * out[5] max |div E - (rho0+rho1)| over physical nodes (Gauss residual) */
 #define PIC_NDIAG 6
 int pic_diagnostics(pic_ctx *ctx, double *out, int n);
+
+/* ---- device-side particle loaders ------------------------------------
+ * Both replace the species' particles like pic_upload_particles, without
+ * host particle memory.
+ *
+ * pic_initialize_particles: initialize_particles (src/particle.cpp:50-111,
+ * declared include/particle.h:32-37) on the device: cbrt(cell_per_particles)
+ * lattice points per cell and axis at xst + i*norm + norm/2 (cell units),
+ * weight density(x*dx, y*dy, z*dz) / cell_per_particles, points with weight
+ * <= 0 skipped, ids 0.. in k, j, i order, momenta initial_p[3], spins
+ * initial_s[3], x_old = 0, the species' charge and mass.  The density
+ * function is data instead of a host callback: a uniform value, a box
+ * (src/constants.cpp:87-101 is the box 5 l0 < x_phys <= 15 l0 on every axis
+ * with value `density`), or a piecewise-linear profile in physical x.      */
+enum { PIC_DENSITY_UNIFORM = 0, PIC_DENSITY_BOX = 1, PIC_DENSITY_XPROFILE = 2 };
+typedef struct PicDensity {
+    int32_t kind;            /* PIC_DENSITY_* */
+    int32_t nknots;          /* XPROFILE: number of knots */
+    double value;            /* UNIFORM / BOX: the density */
+    double lo[3], hi[3];     /* BOX: `value` where lo[d] < coordinate_d * d_d <= hi[d] on every axis, else 0 */
+    const double *knot_x;    /* XPROFILE: ascending physical x of the knots (host memory) */
+    const double *knot_v;    /* XPROFILE: density at the knots; linear between, end values beyond */
+} PicDensity;
+int pic_initialize_particles(pic_ctx *ctx, int kind, const PicDensity *density, int cell_per_particles,
+                             const double *initial_p, const double *initial_s);
+
+/* pic_generate_thermal (no counterpart in the reference, whose loader is
+ * the lattice above): a seeded thermal plasma, ppc particles per cell at
+ * uniform random positions in the cell, momenta N(0, u_th^2) per component,
+ * weight density / ppc, zero spins, ids 0.. in cell order (x fastest).
+ * Counter-based (Philox4x32-10 keyed by seed and kind): the same seed gives
+ * the same particles on any device and in any chunking.                   */
+int pic_generate_thermal(pic_ctx *ctx, int kind, int ppc, double density, double u_th, uint64_t seed);
+
+/* ---- initial electrostatic field (no counterpart in the reference) ----
+ * The reference starts from E = 0 whatever the particles' charge.  This
+ * solves, in FP64 whatever the context precision, A phi = rho - <rho> with
+ * A the 7-point Laplacian of the Yee grid, and sets E = -grad phi on the
+ * faces, Ex(i+1/2) = -(phi(i+1) - phi(i)) / dx (and Ey, Ez), so that the
+ * discrete divergence pic_diagnostics uses equals rho - <rho>.  rho is the
+ * charge density of both species deposited at the current particle
+ * positions with the push's rho shape (src/particle.cpp:503-514) onto the
+ * physical nodes; <rho> is its mean (a uniform neutralising background).
+ * Periodic axes wrap; absorbing axes have E = 0 on the faces outside the
+ * physical nodes (zero flux).  B, J, rho arrays and particles are not
+ * touched.  Conjugate gradients run until ||b - A phi|| <= rel_tol ||b||
+ * or max_iter iterations (PIC_ENOCONV, with E set from the last iterate).
+ * out[0] iterations, out[1] final relative residual, out[2] <rho>,
+ * out[3] max |div E - (rho - <rho>)| over the physical nodes, evaluated
+ * from E as stored (FP32 contexts: after rounding E to FP32). */
+#define PIC_NPOISSON 4
+int pic_solve_initial_field(pic_ctx *ctx, double rel_tol, int max_iter, double *out, int nout);
 
 /* ---- diagnostics without device allocation (no reference counterpart) --
  * For callers that cannot let a library call cudaMalloc (a host code that

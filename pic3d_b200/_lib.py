@@ -12,11 +12,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 # PIC3D_LIBRARY may point at another build of the same sources (tuning builds)
 LIB_PATH = os.environ.get("PIC3D_LIBRARY", os.path.join(HERE, "libpic3d_b200.so"))
 
-PIC_OK, PIC_EINVAL, PIC_ENOMEM, PIC_EOOB, PIC_ENAN, PIC_ETIMEOUT, PIC_ECUDA, PIC_EOVERFLOW, PIC_ERANGE = range(9)
+(PIC_OK, PIC_EINVAL, PIC_ENOMEM, PIC_EOOB, PIC_ENAN, PIC_ETIMEOUT, PIC_ECUDA, PIC_EOVERFLOW, PIC_ERANGE,
+ PIC_ENOCONV) = range(10)
 STATUS_NAMES = {0: "PIC_OK", 1: "PIC_EINVAL", 2: "PIC_ENOMEM", 3: "PIC_EOOB", 4: "PIC_ENAN", 5: "PIC_ETIMEOUT",
-                6: "PIC_ECUDA", 7: "PIC_EOVERFLOW", 8: "PIC_ERANGE"}
+                6: "PIC_ECUDA", 7: "PIC_EOVERFLOW", 8: "PIC_ERANGE", 9: "PIC_ENOCONV"}
 ARRAYS = ["ex", "ey", "ez", "bx", "by", "bz", "jx", "jy", "jz", "rho0", "rho1"]
 NDIAG = 6
+NPOISSON = 4
 
 _I32, _I64, _D = ctypes.c_int32, ctypes.c_int64, ctypes.c_double
 
@@ -35,6 +37,14 @@ class PicParams(ctypes.Structure):
         ("precision", _I32), ("spin", _I32), ("deposit_rho", _I32),
         ("laser_envelope", _I32), ("laser_profile", _I32), ("tile", _I32), ("sort_interval", _I32), ("adjoint", _I32),
     ]
+
+
+class PicDensity(ctypes.Structure):
+    _fields_ = [("kind", _I32), ("nknots", _I32), ("value", _D), ("lo", _D * 3), ("hi", _D * 3),
+                ("knot_x", ctypes.POINTER(_D)), ("knot_v", ctypes.POINTER(_D))]
+
+
+DENSITY_UNIFORM, DENSITY_BOX, DENSITY_XPROFILE = range(3)
 
 
 class PicError(RuntimeError):
@@ -56,7 +66,8 @@ EXPORTS = [
     "pic_checkpoint_restore", "pic_adjoint_tape", "pic_adjoint_record", "pic_adjoint_seed_kinetic",
     "pic_adjoint_backward", "pic_adjoint_weight_grad", "pic_adjoint_profile_grad", "pic_adjoint_release",
     "pic_update_fields_full", "pic_exchange_boundary", "pic_exchange_current", "pic_filter_current",
-    "pic_binomial_filter_currents", "pic_deposit_particle", "pic_eval",
+    "pic_binomial_filter_currents", "pic_deposit_particle", "pic_eval", "pic_solve_initial_field",
+    "pic_initialize_particles", "pic_generate_thermal",
 ]
 
 # pic_eval selectors (include/pic3d_gpu.h)
@@ -117,5 +128,8 @@ def load(path: str = LIB_PATH):
     lib.pic_eval.argtypes = [V, ctypes.c_int, P(_D), ctypes.c_int, P(_D), ctypes.c_int]
     lib.pic_save.argtypes = [V, ctypes.c_char_p]
     lib.pic_load.argtypes = [V, ctypes.c_char_p]
+    lib.pic_solve_initial_field.argtypes = [V, _D, ctypes.c_int, P(_D), ctypes.c_int]
+    lib.pic_initialize_particles.argtypes = [V, ctypes.c_int, P(PicDensity), ctypes.c_int, P(_D), P(_D)]
+    lib.pic_generate_thermal.argtypes = [V, ctypes.c_int, ctypes.c_int, _D, _D, ctypes.c_uint64]
     _lib = lib
     return lib

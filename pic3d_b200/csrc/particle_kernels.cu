@@ -426,6 +426,103 @@ void launch_convert_array(pic_ctx *c, void *dst, const void *src, long long n, i
 }
 
 // ---------------------------------------------------------------------------
+// Device-side particle generators: they write reference records [off,
+// off + n) into a staging buffer, which records_to_soa_kernel then converts
+// (the same path as an upload from host memory).
+
+// initialize_particles (src/particle.cpp:50-111): the lattice points with a
+// positive density, in the reference's k, j, i order.  The density of the
+// supported profiles is positive on a product of per-axis index sets, so
+// the q-th created particle is the q-th point of that product; the host
+// passes the coordinates of the kept indices per axis (ax, ay, az) and the
+// weight per kept x index (wx) or one weight for all (wconst).
+__global__ void lattice_records_kernel(LatticeArgs a) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
+    const long long q = a.off + t;
+    const long long i = q % a.nvx, j = (q / a.nvx) % a.nvy, k = q / (a.nvx * a.nvy);
+    Rec r{};
+    r.id = (int)q;   // my_rank * num_particles + particle_index with rank 0
+    r.x = a.ax[i];
+    r.y = a.ay[j];
+    r.z = a.az[k];
+    r.px = a.p[0];
+    r.py = a.p[1];
+    r.pz = a.p[2];
+    r.sx = a.s[0];
+    r.sy = a.s[1];
+    r.sz = a.s[2];
+    r.gamma = a.gamma;
+    r.charge = a.charge;
+    r.mass = a.mass;
+    r.weight = a.wx ? a.wx[i] : a.wconst;
+    ((Rec *)a.rec)[t] = r;
+}
+
+// Philox4x32-10 (Salmon, Moraes, Dror and Shaw, "Parallel random numbers: as
+// easy as 1, 2, 3", SC 2011): a counter-based generator, 10 rounds of two
+// 32x32->64 multiplies with a Weyl-sequence key schedule.
+__device__ __forceinline__ void philox4x32_10(unsigned (&c)[4], unsigned k0, unsigned k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const unsigned lo0 = 0xD2511F53u * c[0], hi0 = __umulhi(0xD2511F53u, c[0]);
+        const unsigned lo1 = 0xCD9E8D57u * c[2], hi1 = __umulhi(0xCD9E8D57u, c[2]);
+        const unsigned n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+        c[0] = n0;
+        c[1] = lo1;
+        c[2] = n2;
+        c[3] = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+// seeded thermal plasma: ppc particles per cell at uniform random offsets in
+// the cell, momenta N(0, u_th^2) per component (Box-Muller), weight
+// density / ppc, id = index.  Particle q draws two Philox blocks with
+// counters (q, 0) and (q, 1) under key (seed, kind).
+__global__ void thermal_records_kernel(ThermalArgs a) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
+    const long long q = a.off + t;
+    const long long cell = q / a.ppc;
+    const long long cx = cell % a.nx, cy = (cell / a.nx) % a.ny, cz = cell / ((long long)a.nx * a.ny);
+    unsigned u[8];
+    for (int h = 0; h < 2; ++h) {
+        unsigned c[4] = {(unsigned)q, (unsigned)(q >> 32), (unsigned)h, 0u};
+        philox4x32_10(c, a.key0, a.key1);
+        for (int e = 0; e < 4; ++e) u[4 * h + e] = c[e];
+    }
+    const double inv32 = 2.3283064365386963e-10;   // 2^-32
+    Rec r{};
+    r.id = (int)q;
+    r.x = (double)cx + (double)u[0] * inv32;
+    r.y = (double)cy + (double)u[1] * inv32;
+    r.z = (double)cz + (double)u[2] * inv32;
+    // Box-Muller: radius from a uniform in (0, 1], angle from one in [0, 1)
+    const double two_pi = 6.283185307179586;
+    const double r0 = sqrt(-2.0 * log(((double)u[3] + 1.0) * inv32));
+    const double r1 = sqrt(-2.0 * log(((double)u[5] + 1.0) * inv32));
+    const double t0 = two_pi * (double)u[4] * inv32, t1 = two_pi * (double)u[6] * inv32;
+    r.px = a.u_th * r0 * cos(t0);
+    r.py = a.u_th * r0 * sin(t0);
+    r.pz = a.u_th * r1 * cos(t1);
+    r.gamma = sqrt(1.0 + (r.px * r.px + r.py * r.py + r.pz * r.pz));
+    r.charge = a.charge;
+    r.mass = a.mass;
+    r.weight = a.weight;
+    ((Rec *)a.rec)[t] = r;
+}
+
+void launch_lattice_records(pic_ctx *c, const LatticeArgs &a) {
+    if (a.n > 0) lattice_records_kernel<<<(unsigned)((a.n + 255) / 256), 256, 0, c->stream>>>(a);
+}
+
+void launch_thermal_records(pic_ctx *c, const ThermalArgs &a) {
+    if (a.n > 0) thermal_records_kernel<<<(unsigned)((a.n + 255) / 256), 256, 0, c->stream>>>(a);
+}
+
+// ---------------------------------------------------------------------------
 // Deposit of one particle's move from (xo, yo, zo) to (xn, yn, zn), absolute
 // cell coordinates, with charge x weight qw: the reference's
 // currents_particle (src/particle.cpp:372-515) for a single record, through

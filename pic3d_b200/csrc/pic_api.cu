@@ -176,6 +176,48 @@ int sync_status(pic_ctx *c) {
     return PIC_OK;
 }
 
+// Species set-up shared by pic_upload_particles and the device generators:
+// capacity for n particles, cleared sort / removal state, and the staging
+// buffer for one chunk of records.
+int begin_fill(pic_ctx *c, int kind, int64_t n, bool spin_nonzero, double wmax) {
+    Species &s = c->sp[kind];
+    bool want_spin = c->p.spin && c->p.mass[kind] == 1.0;
+    if (n > s.cap || (want_spin && !s.a.sx)) {
+        int r = alloc_species(c, kind, n > c->p.capacity[kind] ? n : c->p.capacity[kind], want_spin);
+        if (r) return r;
+    }
+    s.cur = 0;
+    s.sorted = false;
+    if (s.dead) cudaMemsetAsync(s.dead, 0, (size_t)s.cap, c->stream);
+    s.spin_nonzero = spin_nonzero;
+    s.max_abs_w = wmax;
+    return ensure_stage(c, (size_t)(n < kChunk ? n : kChunk) * 144);
+}
+
+// the count of a filled species, and the compaction lists sized for it
+int end_fill(pic_ctx *c, int kind, int64_t n, const char *what) {
+    Species &s = c->sp[kind];
+    long long cnt = n;
+    CK(cudaMemcpyAsync(s.d_count, &cnt, sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    s.n_host = n;
+    int r = ensure_lists(c, n > c->sp[1 - kind].cap ? n : c->sp[1 - kind].cap);
+    if (r) return r;
+    return launch_check(c, what);
+}
+
+// piecewise-linear density in physical x through the knots, the end values
+// beyond them
+double xprofile(const PicDensity &d, double x) {
+    const int m = d.nknots;
+    if (x <= d.knot_x[0]) return d.knot_v[0];
+    if (x >= d.knot_x[m - 1]) return d.knot_v[m - 1];
+    int k = 1;
+    while (d.knot_x[k] < x) ++k;
+    const double x0 = d.knot_x[k - 1], x1 = d.knot_x[k];
+    return d.knot_v[k - 1] + (d.knot_v[k] - d.knot_v[k - 1]) * ((x - x0) / (x1 - x0));
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -435,18 +477,7 @@ int pic_upload_particles(pic_ctx *c, int kind, const void *records, int64_t n) {
         std::memcpy(s, rec + 144 * i + 80, 24);
         spin_nonzero = spin_nonzero || s[0] != 0.0 || s[1] != 0.0 || s[2] != 0.0;
     }
-    Species &s = c->sp[kind];
-    bool want_spin = c->p.spin && c->p.mass[kind] == 1.0;
-    if (n > s.cap || (want_spin && !s.a.sx)) {
-        int r = alloc_species(c, kind, n > c->p.capacity[kind] ? n : c->p.capacity[kind], want_spin);
-        if (r) return r;
-    }
-    s.cur = 0;
-    s.sorted = false;
-    if (s.dead) cudaMemsetAsync(s.dead, 0, (size_t)s.cap, c->stream);
-    s.spin_nonzero = spin_nonzero;
-    s.max_abs_w = wmax;
-    int r = ensure_stage(c, (size_t)(n < kChunk ? n : kChunk) * 144);
+    int r = begin_fill(c, kind, n, spin_nonzero, wmax);
     if (r) return r;
     for (int64_t off = 0; off < n; off += kChunk) {
         int64_t m = n - off < kChunk ? n - off : kChunk;
@@ -454,13 +485,127 @@ int pic_upload_particles(pic_ctx *c, int kind, const void *records, int64_t n) {
         launch_upload_particles(c, kind, c->d_stage, m, off);
         CK(cudaStreamSynchronize(c->stream));
     }
-    long long cnt = n;
-    CK(cudaMemcpyAsync(s.d_count, &cnt, sizeof(long long), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    s.n_host = n;
-    r = ensure_lists(c, n > c->sp[1 - kind].cap ? n : c->sp[1 - kind].cap);
+    return end_fill(c, kind, n, "pic_upload_particles");
+}
+
+int pic_initialize_particles(pic_ctx *c, int kind, const PicDensity *dens, int cell_per_particles,
+                             const double *initial_p, const double *initial_s) {
+    if (!c || kind < 0 || kind > 1 || !dens || cell_per_particles < 1 || !initial_p || !initial_s) return PIC_EINVAL;
+    cudaSetDevice(c->device);
+    const PicParams &p = c->p;
+    const int n[3] = {p.local_xcells, p.local_ycells, p.local_zcells};
+    const double h[3] = {p.dx, p.dy, p.dz};
+    if (dens->kind == PIC_DENSITY_XPROFILE) {
+        if (dens->nknots < 1 || !dens->knot_x || !dens->knot_v) return fail(c, PIC_EINVAL, "x profile needs knots");
+        for (int k = 1; k < dens->nknots; ++k)
+            if (!(dens->knot_x[k] > dens->knot_x[k - 1])) return fail(c, PIC_EINVAL, "x profile knots must ascend");
+    } else if (dens->kind != PIC_DENSITY_UNIFORM && dens->kind != PIC_DENSITY_BOX) {
+        return fail(c, PIC_EINVAL, "unknown density profile kind");
+    }
+    // lattice of src/particle.cpp:58-63 (one rank: xst = 0, xend = n)
+    std::vector<double> coord[3], wx;
+    for (int d = 0; d < 3; ++d) {
+        const int num = (int)(n[d] * std::cbrt(cell_per_particles));
+        const double xst = 0.0, xend = (double)n[d];
+        const double norm = (xend - xst) / num;
+        for (int i = 0; i < num; ++i) {
+            const double pos = xst + (i) * norm + norm / 2.0;   // particle.cpp:73-75
+            const double phys = pos * h[d];
+            bool keep = true;
+            if (dens->kind == PIC_DENSITY_BOX) keep = phys > dens->lo[d] && phys <= dens->hi[d];
+            if (dens->kind == PIC_DENSITY_XPROFILE && d == 0) {
+                const double v = xprofile(*dens, phys) / cell_per_particles;
+                keep = v > 0.0;
+                if (keep) wx.push_back(v);
+            }
+            if (keep) coord[d].push_back(pos);
+        }
+    }
+    double wconst = 0.0;
+    if (dens->kind != PIC_DENSITY_XPROFILE) {
+        wconst = dens->value / cell_per_particles;
+        if (!(wconst > 0.0))
+            for (auto &v : coord) v.clear();
+    }
+    if (!std::isfinite(wconst)) return fail(c, PIC_EINVAL, "non-finite density");
+    for (double v : wx)
+        if (!std::isfinite(v)) return fail(c, PIC_EINVAL, "non-finite density");
+    const int64_t total = (int64_t)coord[0].size() * (int64_t)coord[1].size() * (int64_t)coord[2].size();
+    const int64_t capacity = (int64_t)n[0] * n[1] * n[2] * cell_per_particles;
+    if (total > capacity || total >= (1ll << 31)) return fail(c, PIC_EINVAL, "too many particles for int ids");
+    double wmax = std::fabs(wconst);
+    for (double v : wx) wmax = std::max(wmax, std::fabs(v));
+    const bool spin_nonzero = initial_s[0] != 0.0 || initial_s[1] != 0.0 || initial_s[2] != 0.0;
+    int r = begin_fill(c, kind, total, spin_nonzero, wmax);
     if (r) return r;
-    return launch_check(c, "pic_upload_particles");
+    // per-axis tables next to the records in one device buffer
+    const size_t tab = coord[0].size() + coord[1].size() + coord[2].size() + wx.size();
+    double *d_tab = nullptr;
+    r = dalloc(c, &d_tab, std::max<size_t>(tab, 1) * sizeof(double));
+    if (r) return r;
+    size_t o = 0;
+    const double *dptr[4];
+    std::vector<double> *src[4] = {&coord[0], &coord[1], &coord[2], &wx};
+    for (int k = 0; k < 4; ++k) {
+        dptr[k] = d_tab + o;
+        if (!src[k]->empty())
+            cudaMemcpyAsync(d_tab + o, src[k]->data(), src[k]->size() * sizeof(double), cudaMemcpyHostToDevice,
+                            c->stream);
+        o += src[k]->size();
+    }
+    LatticeArgs a{};
+    a.ax = dptr[0]; a.ay = dptr[1]; a.az = dptr[2];
+    a.wx = wx.empty() ? nullptr : dptr[3];
+    a.wconst = wconst;
+    a.nvx = (long long)coord[0].size();
+    a.nvy = (long long)coord[1].size();
+    for (int d = 0; d < 3; ++d) { a.p[d] = initial_p[d]; a.s[d] = initial_s[d]; }
+    a.gamma = std::sqrt(1 + (initial_p[0] * initial_p[0] + initial_p[1] * initial_p[1] + initial_p[2] * initial_p[2]));
+    a.charge = p.charge[kind];
+    a.mass = p.mass[kind];
+    a.rec = c->d_stage;
+    cudaError_t e = cudaSuccess;
+    for (int64_t off = 0; off < total && e == cudaSuccess; off += kChunk) {
+        a.off = off;
+        a.n = total - off < kChunk ? total - off : kChunk;
+        launch_lattice_records(c, a);
+        launch_upload_particles(c, kind, c->d_stage, a.n, off);
+        e = cudaStreamSynchronize(c->stream);
+    }
+    cudaFree(d_tab);
+    CK(e);
+    return end_fill(c, kind, total, "pic_initialize_particles");
+}
+
+int pic_generate_thermal(pic_ctx *c, int kind, int ppc, double density, double u_th, uint64_t seed) {
+    if (!c || kind < 0 || kind > 1 || ppc < 1 || !(density > 0.0) || !(u_th >= 0.0) || !std::isfinite(u_th))
+        return PIC_EINVAL;
+    cudaSetDevice(c->device);
+    const PicParams &p = c->p;
+    const int64_t total = (int64_t)p.local_xcells * p.local_ycells * p.local_zcells * ppc;
+    if (total >= (1ll << 31)) return fail(c, PIC_EINVAL, "too many particles for int ids");
+    const double w = density / ppc;
+    int r = begin_fill(c, kind, total, false, w);
+    if (r) return r;
+    ThermalArgs a{};
+    a.nx = p.local_xcells;
+    a.ny = p.local_ycells;
+    a.ppc = ppc;
+    a.key0 = (unsigned)seed;
+    a.key1 = (unsigned)(seed >> 32) ^ (0x9E3779B9u * (unsigned)(kind + 1));
+    a.u_th = u_th;
+    a.weight = w;
+    a.charge = p.charge[kind];
+    a.mass = p.mass[kind];
+    a.rec = c->d_stage;
+    for (int64_t off = 0; off < total; off += kChunk) {
+        a.off = off;
+        a.n = total - off < kChunk ? total - off : kChunk;
+        launch_thermal_records(c, a);
+        launch_upload_particles(c, kind, c->d_stage, a.n, off);
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return end_fill(c, kind, total, "pic_generate_thermal");
 }
 
 int pic_download_particles(pic_ctx *c, int kind, void *records, int64_t cap, int64_t *n) {

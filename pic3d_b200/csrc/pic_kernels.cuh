@@ -19,6 +19,26 @@ void launch_binomial_pass(pic_ctx *c, int ring_index, int axis, void *scratch);
 int launch_eval(pic_ctx *c, int what, const double *in, double *d_out);
 
 // particle_kernels.cu
+// device generators of reference records (staging buffer `rec`, records
+// [off, off + n) of the species)
+struct LatticeArgs {
+    void *rec;
+    long long n, off;
+    const double *ax, *ay, *az;   // coordinates of the kept lattice indices per axis
+    const double *wx;             // weight per kept x index, or null: wconst
+    double wconst;
+    long long nvx, nvy;
+    double p[3], s[3], gamma, charge, mass;
+};
+struct ThermalArgs {
+    void *rec;
+    long long n, off;
+    int nx, ny, ppc;
+    unsigned key0, key1;
+    double u_th, weight, charge, mass;
+};
+void launch_lattice_records(pic_ctx *c, const LatticeArgs &a);
+void launch_thermal_records(pic_ctx *c, const ThermalArgs &a);
 void launch_push(pic_ctx *c, int kind);
 void launch_push_list(pic_ctx *c, int kind, const int *idx, const unsigned long long *count);
 void launch_remove(pic_ctx *c, int kind);

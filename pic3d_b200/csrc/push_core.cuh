@@ -176,6 +176,26 @@ struct FixedAcc {
     }
 };
 
+// The middle loop of a current component over m = 0 .. len-1 (len <= P+1),
+// calling body(m, s0[m], ds[m]): fully unrolled, or rolled with the two
+// weights picked from registers.
+template <bool ROLL, int P, typename real, class F>
+__device__ __forceinline__ void mid_loop(int len, const real (&s0)[P + 1], const real (&ds)[P + 1], F &&body) {
+    if constexpr (ROLL) {
+#pragma unroll 1
+        for (int m = 0; m <= P; ++m) {
+            if (m >= len) break;
+            body(m, pick(s0, m), pick(ds, m));
+        }
+    } else {
+#pragma unroll
+        for (int m = 0; m <= P; ++m) {
+            if (m >= len) break;
+            body(m, s0[m], ds[m]);
+        }
+    }
+}
+
 // Esirkepov deposit (src/particle.cpp:427-500) and rho (:503-514).  The
 // last point of each running sum (the sum of all ds, zero up to rounding)
 // is not added.
@@ -199,6 +219,10 @@ __device__ __forceinline__ void deposit(const Acc &acc, const real (&dxdt)[3], c
     const real cx = qw * dxdt[0] * acc.coef(0), cy = qw * dxdt[1] * acc.coef(1), cz = qw * dxdt[2] * acc.coef(2);
     const int rx = acc.sy, rxy = acc.sz;
     const int r0 = base[2] * rxy + base[1] * rx + base[0] + acc.o;
+    // The middle loops stay rolled for FP32 at 4th order: its fully unrolled
+    // code overflows the instruction cache (measured 10 % faster rolled),
+    // while FP64 and 2nd order run faster unrolled.
+    constexpr bool kRollMid = sizeof(real) == 4 && P == 5;
     // a particle that did not move (every ds zero) adds no current
     bool moved = false;
 #pragma unroll
@@ -208,10 +232,8 @@ __device__ __forceinline__ void deposit(const Acc &acc, const real (&dxdt)[3], c
 #pragma unroll 1
         for (int k = 0; k < len[2]; ++k) {
             const real s0z = pick(s0[2], k), dsz = pick(ds[2], k);
-#pragma unroll
-            for (int j = 0; j <= P; ++j) {
-                if (j >= len[1]) break;
-                real wyz = s0[1][j] * s0z + half * ds[1][j] * s0z + half * s0[1][j] * dsz + third * ds[1][j] * dsz;
+            mid_loop<kRollMid, P>(len[1], s0[1], ds[1], [&](int j, real s0y, real dsy) {
+                const real wyz = s0y * s0z + half * dsy * s0z + half * s0y * dsz + third * dsy * dsz;
                 const real cw = -cx * wyz;
                 real a = 0;
                 const int row = r0 + k * rxy + j * rx;
@@ -221,16 +243,14 @@ __device__ __forceinline__ void deposit(const Acc &acc, const real (&dxdt)[3], c
                     a += ds[0][i];
                     acc.add(0, row + i, cw * a);
                 }
-            }
+            });
         }
         // Jy
 #pragma unroll 1
         for (int k = 0; k < len[2]; ++k) {
             const real s0z = pick(s0[2], k), dsz = pick(ds[2], k);
-#pragma unroll
-            for (int i = 0; i <= P; ++i) {
-                if (i >= len[0]) break;
-                real wxz = s0[0][i] * s0z + half * ds[0][i] * s0z + half * s0[0][i] * dsz + third * ds[0][i] * dsz;
+            mid_loop<kRollMid, P>(len[0], s0[0], ds[0], [&](int i, real s0x, real dsx) {
+                const real wxz = s0x * s0z + half * dsx * s0z + half * s0x * dsz + third * dsx * dsz;
                 const real cw = -cy * wxz;
                 real a = 0;
                 const int col = r0 + k * rxy + i;
@@ -240,16 +260,14 @@ __device__ __forceinline__ void deposit(const Acc &acc, const real (&dxdt)[3], c
                     a += ds[1][j];
                     acc.add(1, col + j * rx, cw * a);
                 }
-            }
+            });
         }
         // Jz
 #pragma unroll 1
         for (int j = 0; j < len[1]; ++j) {
             const real s0y = pick(s0[1], j), dsy = pick(ds[1], j);
-#pragma unroll
-            for (int i = 0; i <= P; ++i) {
-                if (i >= len[0]) break;
-                real wxy = s0[0][i] * s0y + half * ds[0][i] * s0y + half * s0[0][i] * dsy + third * ds[0][i] * dsy;
+            mid_loop<kRollMid, P>(len[0], s0[0], ds[0], [&](int i, real s0x, real dsx) {
+                const real wxy = s0x * s0y + half * dsx * s0y + half * s0x * dsy + third * dsx * dsy;
                 const real cw = -cz * wxy;
                 real a = 0;
                 const int col = r0 + j * rx + i;
@@ -259,7 +277,7 @@ __device__ __forceinline__ void deposit(const Acc &acc, const real (&dxdt)[3], c
                     a += ds[2][k];
                     acc.add(2, col + k * rxy, cw * a);
                 }
-            }
+            });
         }
     }
     if (acc.has_rho()) {

@@ -220,6 +220,43 @@ class Simulation:
         return dict(field_energy=out[0], kinetic0=out[1], kinetic1=out[2], charge0=out[3], charge1=out[4],
                     gauss_max=out[5])
 
+    def initialize_particles(self, kind: int, cell_per_particles: int, density="uniform", value: float = 1.0,
+                             lo=(0.0, 0.0, 0.0), hi=(0.0, 0.0, 0.0), knots=None,
+                             initial_p=(0.0, 0.0, 0.0), initial_s=(0.0, 0.0, 0.0)):
+        """The reference's lattice loader on the device (pic_initialize_particles).
+        density: "uniform" (value), "box" (value where lo < x*dx <= hi per
+        axis) or "xprofile" (knots = (x_phys array, density array))."""
+        d = L.PicDensity()
+        d.kind = {"uniform": L.DENSITY_UNIFORM, "box": L.DENSITY_BOX, "xprofile": L.DENSITY_XPROFILE}[density]
+        d.value = value
+        for k in range(3):
+            d.lo[k], d.hi[k] = lo[k], hi[k]
+        keep = []
+        if density == "xprofile":
+            kx = np.ascontiguousarray(knots[0], dtype=np.float64)
+            kv = np.ascontiguousarray(knots[1], dtype=np.float64)
+            keep = [kx, kv]
+            d.nknots = len(kx)
+            d.knot_x = kx.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            d.knot_v = kv.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        p0 = (ctypes.c_double * 3)(*initial_p)
+        s0 = (ctypes.c_double * 3)(*initial_s)
+        self._check(self.lib.pic_initialize_particles(self.ctx, kind, ctypes.byref(d), cell_per_particles, p0, s0))
+        del keep
+
+    def generate_thermal(self, kind: int, ppc: int, density: float, u_th: float, seed: int):
+        """Seeded thermal plasma generated on the device (pic_generate_thermal)."""
+        self._check(self.lib.pic_generate_thermal(self.ctx, kind, ppc, density, u_th, seed))
+
+    def solve_initial_field(self, rel_tol: float = 1e-10, max_iter: int = 50000) -> dict:
+        """FP64 Poisson solve for the initial E of the current particles
+        (pic_solve_initial_field): div E = rho - <rho>.  The relative
+        residual cannot go much below 1e-13 (FP64 rounding); a smaller
+        rel_tol ends with PIC_ENOCONV."""
+        out = (ctypes.c_double * L.NPOISSON)()
+        self._check(self.lib.pic_solve_initial_field(self.ctx, rel_tol, max_iter, out, L.NPOISSON))
+        return dict(iterations=int(out[0]), rel_residual=out[1], mean_rho=out[2], gauss_max=out[3])
+
     # -- profiling ------------------------------------------------------------------
     def profile(self, on: bool = True):
         self._check(self.lib.pic_profile_enable(self.ctx, 1 if on else 0))
