@@ -323,6 +323,41 @@ def adjoint_bench(steps=600, short_steps=100):
                     "at the absorbing faces)"}
 
 
+def scaleup_bench(local, steps=3, warmup=3):
+    """Throughput scale-up configuration: periodic 512 x 256 x 256 thermal
+    electron-proton plasma, 8 particles per cell per species (536,870,912
+    particles), u_th = 0.02, 2nd- and 4th-order shapes, FP32 and FP64.
+    Particles come from the device generator (pic_generate_thermal: seeded
+    Philox, no host particle memory); a short timed window per case keeps
+    the default run within minutes (the per-step cost is steady: no laser,
+    uniform plasma)."""
+    from pic3d_b200 import workloads as W
+    from pic3d_b200.simulation import Simulation
+    out = []
+    for mem in (2, 4):
+        for prec in ("fp32", "fp64"):
+            w = W.thermal_scaleup(mem=mem, precision=prec)
+            sim = Simulation(w, precision=prec, device=local, **TILE)
+            for k in range(2):
+                sim.generate_thermal(k, 8, 1.0, 0.02, 97 + k)
+            npart = sum(sim.num_particles(k) for k in range(2))
+            sim.initial_push()
+            sim.run_main_time_loop(warmup)
+            ms, kern = timed_steps(sim, steps, prof=True)
+            sim.close()
+            tile = kern.get("tile_push_gather_deposit", (0.0, 1))
+            avg = tile[0] / max(tile[1], 1)
+            ncell = w.nx * w.ny * w.nz
+            per = BYTES_PER_PARTICLE[prec] + GRID_BYTES_PER_CELL[prec] * ncell / npart
+            peak, _ = measured_peaks()
+            out.append({"order": 2 if mem == 2 else 4, "precision": prec, "particles": npart,
+                        "particle_steps_per_s": npart * steps / (ms / 1e3), "ms_per_step": ms / steps,
+                        "cell_updates_per_s": ncell * steps / (ms / 1e3), "tile_push_ms": avg,
+                        "tile_push_roofline_frac": per * npart / (avg / 1e3) / 1e9 / peak if avg > 0 else None})
+    return {"workload": "thermal_scaleup_512x256x256", "cells": [512, 256, 256], "particles_per_cell": 16,
+            "u_th": 0.02, "steps": steps, "warmup": warmup, "results": out}
+
+
 def field_rel_err(a: dict, b: dict):
     num = sum(float(np.sum((a[n] - b[n]) ** 2)) for n in ("ex", "ey", "ez", "bx", "by", "bz"))
     den = sum(float(np.sum(b[n] ** 2)) for n in ("ex", "ey", "ez", "bx", "by", "bz"))
@@ -341,6 +376,7 @@ def main():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-scaleup", action="store_true")
     ap.add_argument("--adjoint-steps", type=int, default=600)
     ap.add_argument("--tile", type=int, default=0, help="shared-memory tile edge (0 default, -1 global kernel)")
     ap.add_argument("--sort-interval", type=int, default=0)
@@ -470,6 +506,12 @@ def main():
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "note": "pic_upload_* of the initial state from host memory, the t=0 push, K pic_run_steps(1) "
                        "each followed by a pic_diagnostics read-back, pic_download_* of the final state"}
+
+    if not args.no_scaleup:
+        try:
+            extra["scaleup"] = scaleup_bench(local)
+        except Exception as e:
+            extra["scaleup"] = {"error": str(e)[:300]}
 
     if rank == 0 and not args.no_adjoint:
         try:

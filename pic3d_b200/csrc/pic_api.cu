@@ -335,7 +335,7 @@ int pic_create(const PicParams *pp, int device, pic_ctx **out) {
     c->sort_interval = p.sort_interval > 0 ? p.sort_interval : 4;
     if (c->tile > 0) {
         for (int d = 0; d < 3; ++d) c->ntile[d] = (n[d] + c->tile - 1) / c->tile;
-        c->nkeys = (long long)c->ntile[0] * c->ntile[1] * c->ntile[2] * c->tile * c->tile * c->tile;
+        c->nkeys = (long long)c->ntile[0] * c->ntile[1] * c->ntile[2] * kOctants * c->tile * c->tile * c->tile;
         if (c->nkeys >= (1ll << 31)) return bad("too many sort keys");
         if (tile_smem_bytes(c) > 227 * 1024) return bad("tile too large for shared memory");
     }

@@ -103,6 +103,9 @@ struct PartArrays {
     int *id = nullptr;
 };
 
+// half-cell octants per cell in the particle sort key (tile, octant, cell)
+constexpr int kOctants = 8;
+
 struct Species {
     int64_t cap = 0;
     int64_t n_host = 0;      // host copy of the count (upper bound between syncs)
@@ -169,7 +172,7 @@ struct pic_ctx {
     // tiling / sorting
     int tile = 0;                        // tile edge in cells (0: global-memory kernel only)
     int ntile[3] = {0, 0, 0};
-    long long nkeys = 0;                 // ntiles * tile^3
+    long long nkeys = 0;                 // ntiles * kOctants * tile^3
     unsigned *d_hist = nullptr;          // nkeys + 1
     unsigned *d_blocksums = nullptr;
     unsigned long long *d_nstrag = nullptr;   // straggler counts, one per species

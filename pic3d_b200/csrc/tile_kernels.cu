@@ -1,7 +1,9 @@
 // Tiled gather + push + deposit with shared-memory staging.
 //
-// Particles of each species are kept in counting-sort order by cell, with
-// cells numbered tile-major (a tile is T^3 cells).  One CTA owns one tile:
+// Particles of each species are kept in counting-sort order by tile (T^3
+// cells), then by half-cell octant of the position (which side of the cell
+// centre on each axis: it fixes the primal stencil index relative to the
+// cell), then by cell.  One CTA owns one tile:
 //   1. it stages the six field components of the tile plus the gather halo
 //      (T + 2H + 1 points per axis) in shared memory,
 //   2. clears shared-memory accumulators for jx, jy, jz, rho0, rho1 over the
@@ -13,9 +15,9 @@
 //   4. flushes the accumulators with one coalesced pass of global atomics
 //      (zero entries skipped); halos of neighbouring tiles overlap, hence the
 //      atomics.
-// Lanes of a warp take particles from 32 different chunks of the tile's
-// cell-sorted list, so they sit in different cells and their shared-memory
-// addresses rarely collide.
+// A warp takes 32 consecutive particles of the sorted list: mostly one
+// octant and consecutive cells, so at a common stencil point their
+// shared-memory addresses fall in different banks.
 //
 // The counting sort (key histogram, exclusive scan, scatter into the second
 // set of arrays) runs every `sort_interval` pushes and after an upload.
@@ -53,21 +55,26 @@ __host__ __device__ constexpr int gather_extent(int T) { return T + 2 * (P / 2) 
 template <int P>
 __host__ __device__ constexpr int deposit_extent(int T) { return T + 2 * (P / 2) + 3; }
 
-__device__ __forceinline__ int cell_key(const TileGeom &t, int cx, int cy, int cz) {
+// Sort key of a particle in cell (cx, cy, cz) whose position in the cell
+// lies in half-cell octant `oct` (bit d set: offset >= 1/2 along axis d, so
+// its primal stencil index is the cell's plus one along d): tile, then
+// octant, then cell within the tile.
+__device__ __forceinline__ int cell_key(const TileGeom &t, int cx, int cy, int cz, int oct) {
     const int T = t.T;
     int tx = cx / T, ty = cy / T, tz = cz / T;
     int lx = cx - tx * T, ly = cy - ty * T, lz = cz - tz * T;
-    return (((tz * t.nt[1] + ty) * t.nt[0] + tx) * T + lz) * T * T + ly * T + lx;
+    return ((((tz * t.nt[1] + ty) * t.nt[0] + tx) * kOctants + oct) * T + lz) * T * T + ly * T + lx;
 }
 
 // cell of a particle for sorting (FP64: periodic wrap as the next push
 // will apply it; clamped into the domain)
 __device__ __forceinline__ int particle_key(const Geom &g, const TileGeom &t, const CellPack &cp, int fp32,
                                             const double *x, const double *y, const double *z, const int *cell,
-                                            long long i) {
-    int c[3];
+                                            const float *ox, const float *oy, const float *oz, long long i) {
+    int c[3], oct = 0;
     if (fp32) {
         cp.unpack(cell[i], c[0], c[1], c[2]);
+        oct = (ox[i] >= 0.5f ? 1 : 0) | (oy[i] >= 0.5f ? 2 : 0) | (oz[i] >= 0.5f ? 4 : 0);
     } else {
         double v[3] = {x[i], y[i], z[i]};
 #pragma unroll
@@ -76,12 +83,14 @@ __device__ __forceinline__ int particle_key(const Geom &g, const TileGeom &t, co
                 if (v[d] < 0.0) v[d] += g.n[d];
                 if (v[d] > (double)g.n[d]) v[d] -= g.n[d];
             }
-            c[d] = (int)floor(v[d]);
+            const double f = floor(v[d]);
+            c[d] = (int)f;
+            oct |= (v[d] - f >= 0.5 ? 1 : 0) << d;
         }
     }
 #pragma unroll
     for (int d = 0; d < 3; ++d) c[d] = min(max(c[d], 0), g.n[d] - 1);
-    return cell_key(t, c[0], c[1], c[2]);
+    return cell_key(t, c[0], c[1], c[2], oct);
 }
 
 // ---------------------------------------------------------------------------
@@ -95,6 +104,7 @@ struct SortArgs {
     const long long *count;
     const double *x, *y, *z;
     const int *cell;
+    const float *ox, *oy, *oz;
     int *keys;
     unsigned *hist;
 };
@@ -104,7 +114,7 @@ __global__ void sort_keys_kernel(SortArgs a) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned act = __ballot_sync(0xffffffffu, i < n);
     if (i >= n) return;
-    int key = particle_key(a.g, a.t, a.cp, a.fp32, a.x, a.y, a.z, a.cell, i);
+    int key = particle_key(a.g, a.t, a.cp, a.fp32, a.x, a.y, a.z, a.cell, a.ox, a.oy, a.oz, i);
     a.keys[i] = key;
     unsigned peers = __match_any_sync(act, key);
     int lane = threadIdx.x & 31;
@@ -267,6 +277,7 @@ void launch_sort(pic_ctx *c, int kind) {
     a.count = s.d_count;
     a.x = s.a.x[s.cur]; a.y = s.a.y[s.cur]; a.z = s.a.z[s.cur];
     a.cell = s.a.cell[s.cur];
+    a.ox = s.a.ox[s.cur]; a.oy = s.a.oy[s.cur]; a.oz = s.a.oz[s.cur];
     a.keys = s.keys;
     a.hist = c->d_hist;
     unsigned nb = (unsigned)((n + 255) / 256);
@@ -365,7 +376,7 @@ __global__ void __launch_bounds__(256, tile_min_blocks<real>()) tile_push_kernel
         dO[d] = t0[d] + g.mem - 2 - H;   // buffer coordinate of the first accumulator point
     }
     // particle ranges of this tile
-    const long long T3 = (long long)T * T * T;
+    const long long T3 = (long long)T * T * T * kOctants;   // keys per tile
     long long pa[2] = {0, 0}, pb[2] = {0, 0};
     long long mtot = 0;
 #pragma unroll
@@ -399,12 +410,10 @@ __global__ void __launch_bounds__(256, tile_min_blocks<real>()) tile_push_kernel
 #pragma unroll
     for (int c = 0; c < 6; ++c) fs[c] = View<const real>{sf + c * GS, gsy, gsz, -(gO[2] * gsz + gO[1] * gsy + gO[0])};
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    // lanes take 32 consecutive chunks of the cell-sorted list (about one
-    // cell each); with more than 32 cells per tile the warps split over
-    // npass groups of 32 chunks
-    const int ncell_t = T * T * T;
-    const int npass = ncell_t > 32 ? (ncell_t / 32 < nwarp ? ncell_t / 32 : nwarp) : 1;
-    const int pass = warp % npass, r0 = warp / npass, rstep = nwarp / npass;
+    // a warp takes 32 consecutive particles of the tile's list: mostly one
+    // octant, so the lanes' primal stencils sit at the same offset from
+    // their cells and their shared-memory accesses at a common stencil point
+    // fall in different banks (the padded strides)
     const int lo_id[3] = {t0[0] + g.mem - 1, t0[1] + g.mem - 1, t0[2] + g.mem - 1};
 
     // 3. particles of both species
@@ -413,7 +422,6 @@ __global__ void __launch_bounds__(256, tile_min_blocks<real>()) tile_push_kernel
         if (pb[k] <= pa[k]) continue;
         const PushArgs<real> &a = ta.sp[k];
         const long long m = pb[k] - pa[k];
-        const long long chunk = (m + 32 * npass - 1) / (32 * npass);
         FixedAcc<real, NL> af;
 #pragma unroll
         for (int c = 0; c < 3; ++c) af.p[c] = sa + c * NL * DS;
@@ -425,8 +433,8 @@ __global__ void __launch_bounds__(256, tile_min_blocks<real>()) tile_push_kernel
 #pragma unroll
         for (int c = 0; c < 4; ++c) af.scale[c] = ta.scale[c];
 #pragma unroll 1
-        for (long long r = r0; r < chunk; r += rstep) {
-            const long long idx = (long long)(pass * 32 + lane) * chunk + r;
+        for (long long base = (long long)warp * 32; base < m; base += (long long)nwarp * 32) {
+            const long long idx = base + lane;
             if (idx >= m) continue;
             const long long p = pa[k] + idx;
             OldPos<real> o;
