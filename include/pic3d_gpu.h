@@ -96,7 +96,11 @@ int pic_download_array(pic_ctx *ctx, int which, double *host);
 
 /* Particles of species `kind` as reference 144-byte records (particle.h:9-29).
  * Upload replaces the species' particles; every record must carry the
- * species' charge and mass.  Download writes at most `cap` records and the
+ * species' charge and mass and a finite weight (checked on the device while
+ * converting: a bad record returns PIC_EINVAL and leaves the species empty).
+ * Both directions stream through pinned host buffers owned by the context,
+ * the host copy of one chunk overlapping the transfer of the next; the
+ * caller's buffer may be ordinary (pageable) memory.  Download writes at most `cap` records and the
  * count to *n; order is the device order (records keep their id), gamma is
  * recomputed from the momentum as the push does (particle.cpp:309-311) and
  * x_old..z_old are the positions before the last push (particle.cpp:267-269). */

@@ -272,6 +272,10 @@ struct ConvArgs {
     void *px, *py, *pz, *w, *sx, *sy, *sz;
     int *id;
     double charge, mass;
+    // upload checks (null: none): check[0] |= 1 charge/mass differ from the
+    // species', 2 non-finite weight, 4 non-zero spin; check[1] = max |weight|
+    // as the bits of a non-negative double
+    unsigned long long *check;
 };
 
 __device__ void to_cell(const Geom &g, const CellPack &cp, int per_wrap, double x, double y, double z, int &cell,
@@ -296,6 +300,27 @@ __device__ void to_cell(const Geom &g, const CellPack &cp, int per_wrap, double 
 
 __global__ void records_to_soa_kernel(ConvArgs a) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (a.check) {
+        // warp-reduced record checks (every lane takes part, in range or not)
+        unsigned long long f = 0, wb = 0;
+        if (t < a.n) {
+            const Rec &q = a.rec[t];
+            if (q.charge != a.charge || q.mass != a.mass) f |= 1ull;
+            if (!isfinite(q.weight)) f |= 2ull;
+            else wb = (unsigned long long)__double_as_longlong(fabs(q.weight));
+            if (q.sx != 0.0 || q.sy != 0.0 || q.sz != 0.0) f |= 4ull;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            f |= __shfl_xor_sync(0xffffffffu, f, o);
+            const unsigned long long v = __shfl_xor_sync(0xffffffffu, wb, o);
+            wb = v > wb ? v : wb;
+        }
+        if ((threadIdx.x & 31) == 0) {
+            if (f) atomicOr(a.check, f);
+            if (wb) atomicMax(a.check + 1, wb);
+        }
+    }
     if (t >= a.n) return;
     const Rec r = a.rec[t];
     long long i = a.off + t;
@@ -399,9 +424,11 @@ static ConvArgs conv_args(pic_ctx *c, int kind, void *rec, int64_t n, int64_t of
     return a;
 }
 
-void launch_upload_particles(pic_ctx *c, int kind, const void *d_records, int64_t n, int64_t offset) {
+void launch_upload_particles(pic_ctx *c, int kind, const void *d_records, int64_t n, int64_t offset,
+                             unsigned long long *check) {
     if (n <= 0) return;
     ConvArgs a = conv_args(c, kind, (void *)d_records, n, offset);
+    a.check = check;
     records_to_soa_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(a);
 }
 

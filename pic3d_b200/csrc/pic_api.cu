@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "pic_kernels.cuh"
@@ -141,6 +142,60 @@ int ensure_lists(pic_ctx *c, int64_t n) {
 }
 
 const int64_t kChunk = 1 << 20;  // particle records staged per copy
+const int64_t kPinRecords = 1 << 18;   // records per pinned host staging buffer (37.7 MB)
+
+// the two pinned staging buffers, at least min(n, kPinRecords) records
+// each, and their events (allocated on first use, grown when needed)
+int ensure_pinned(pic_ctx *c, int64_t n) {
+    const int64_t want = n < kPinRecords ? (n > 0 ? n : 1) : kPinRecords;
+    if (c->pin_records < want) {
+        for (int b = 0; b < 2; ++b) {
+            if (c->h_pin[b]) {
+                if (c->pin_ev[b]) cudaEventSynchronize(c->pin_ev[b]);
+                cudaFreeHost(c->h_pin[b]);
+                c->h_pin[b] = nullptr;
+            }
+        }
+        c->pin_records = 0;
+        for (int b = 0; b < 2; ++b) {
+            cudaError_t e = cudaHostAlloc(&c->h_pin[b], (size_t)want * 144, cudaHostAllocDefault);
+            if (e != cudaSuccess) {
+                c->h_pin[b] = nullptr;
+                return fail(c, PIC_ENOMEM, std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+            }
+        }
+        c->pin_records = want;
+    }
+    for (int b = 0; b < 2; ++b) {
+        if (!c->pin_ev[b]) {
+            cudaError_t e = cudaEventCreateWithFlags(&c->pin_ev[b], cudaEventDisableTiming);
+            if (e != cudaSuccess) {
+                c->pin_ev[b] = nullptr;
+                return fail(c, PIC_ECUDA, std::string("cudaEventCreate: ") + cudaGetErrorString(e));
+            }
+        }
+    }
+    return PIC_OK;
+}
+
+// memcpy of a large block split over a few host threads (host copies into
+// and out of the pinned buffers run at several times one core's rate)
+void par_memcpy(void *dst, const void *src, size_t bytes) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nt = bytes >= (4u << 20) ? (int)std::min(8u, hw > 0 ? hw : 1u) : 1;
+    if (nt <= 1) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t part = ((bytes + nt - 1) / nt + 63) & ~(size_t)63;
+    std::thread th[8];
+    for (int t = 1; t < nt; ++t) {
+        const size_t lo = std::min(bytes, part * t), hi = std::min(bytes, part * (t + 1));
+        th[t] = std::thread([=] { std::memcpy((char *)dst + lo, (const char *)src + lo, hi - lo); });
+    }
+    std::memcpy(dst, src, std::min(bytes, part));
+    for (int t = 1; t < nt; ++t) th[t].join();
+}
 
 int array_info(const pic_ctx *c, int which, void **dptr, long long *n) {
     if (which < 0 || which >= PIC_NARRAYS) return PIC_EINVAL;
@@ -401,6 +456,10 @@ int pic_destroy(pic_ctx *c) {
     for (void *p : c->ring)
         if (p) cudaFree(p);
     for (auto &s : c->sp) free_species(s);
+    for (int b = 0; b < 2; ++b) {
+        if (c->h_pin[b]) cudaFreeHost(c->h_pin[b]);
+        if (c->pin_ev[b]) cudaEventDestroy(c->pin_ev[b]);
+    }
     void *ptrs[] = {c->d_status, c->d_gtab, c->d_profile, c->d_stage, c->d_scratch_ll, c->d_list, c->d_diag,
                     c->d_hist, c->d_blocksums, c->d_nstrag};
     for (void *p : ptrs)
@@ -462,29 +521,40 @@ int pic_upload_particles(pic_ctx *c, int kind, const void *records, int64_t n) {
     if (!c || kind < 0 || kind > 1 || n < 0 || (n > 0 && !records)) return PIC_EINVAL;
     cudaSetDevice(c->device);
     const char *rec = (const char *)records;
-    // every record of a species must carry the species' charge and mass
-    bool spin_nonzero = false;
-    double wmax = 0.0;
-    for (int64_t i = 0; i < n; ++i) {
-        double q, m, s[3], wt;
-        std::memcpy(&wt, rec + 144 * i + 128, 8);
-        if (!std::isfinite(wt)) return fail(c, PIC_EINVAL, "non-finite particle weight");
-        wmax = std::max(wmax, std::fabs(wt));
-        std::memcpy(&q, rec + 144 * i + 112, 8);
-        std::memcpy(&m, rec + 144 * i + 120, 8);
-        if (q != c->p.charge[kind] || m != c->p.mass[kind])
-            return fail(c, PIC_EINVAL, "particle record charge/mass differs from the species parameters");
-        std::memcpy(s, rec + 144 * i + 80, 24);
-        spin_nonzero = spin_nonzero || s[0] != 0.0 || s[1] != 0.0 || s[2] != 0.0;
-    }
-    int r = begin_fill(c, kind, n, spin_nonzero, wmax);
+    int r = begin_fill(c, kind, n, false, 0.0);
     if (r) return r;
-    for (int64_t off = 0; off < n; off += kChunk) {
-        int64_t m = n - off < kChunk ? n - off : kChunk;
-        CK(cudaMemcpyAsync(c->d_stage, rec + 144 * off, (size_t)m * 144, cudaMemcpyHostToDevice, c->stream));
-        launch_upload_particles(c, kind, c->d_stage, m, off);
-        CK(cudaStreamSynchronize(c->stream));
+    r = ensure_pinned(c, n);
+    if (r) return r;
+    // the records' checks (charge and mass equal to the species', finite
+    // weights, any non-zero spin, largest |weight|) run in the conversion
+    // kernel: two words of device scratch
+    unsigned long long *chk = (unsigned long long *)(c->d_scratch_ll + 4);
+    CK(cudaMemsetAsync(chk, 0, 2 * sizeof(unsigned long long), c->stream));
+    // pipeline: the host copy of chunk i into pinned buffer i % 2 overlaps
+    // the DMA and conversion of chunk i - 1
+    int64_t i = 0;
+    for (int64_t off = 0; off < n; off += kPinRecords, ++i) {
+        const int64_t m = n - off < kPinRecords ? n - off : kPinRecords;
+        const int b = (int)(i & 1);
+        CK(cudaEventSynchronize(c->pin_ev[b]));
+        par_memcpy(c->h_pin[b], rec + 144 * off, (size_t)m * 144);
+        CK(cudaMemcpyAsync(c->d_stage, c->h_pin[b], (size_t)m * 144, cudaMemcpyHostToDevice, c->stream));
+        launch_upload_particles(c, kind, c->d_stage, m, off, chk);
+        CK(cudaEventRecord(c->pin_ev[b], c->stream));
     }
+    unsigned long long hc[2] = {0, 0};
+    CK(cudaMemcpyAsync(hc, chk, sizeof(hc), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (hc[0] & 3ull) {
+        // a bad record leaves the species empty
+        r = end_fill(c, kind, 0, "pic_upload_particles");
+        if (r) return r;
+        return fail(c, PIC_EINVAL, (hc[0] & 1ull) ? "particle record charge/mass differs from the species parameters"
+                                                 : "non-finite particle weight");
+    }
+    Species &s = c->sp[kind];
+    s.spin_nonzero = (hc[0] & 4ull) != 0;
+    std::memcpy(&s.max_abs_w, &hc[1], sizeof(double));
     return end_fill(c, kind, n, "pic_upload_particles");
 }
 
@@ -618,14 +688,26 @@ int pic_download_particles(pic_ctx *c, int kind, void *records, int64_t cap, int
     *n = cnt;
     if (cnt > cap) return fail(c, PIC_EINVAL, "download buffer too small");
     if (cnt == 0) return st;
-    int r = ensure_stage(c, (size_t)(cnt < kChunk ? cnt : kChunk) * 144);
+    int r = ensure_stage(c, (size_t)(cnt < kPinRecords ? cnt : kPinRecords) * 144);
+    r = r ? r : ensure_pinned(c, cnt);
     if (r) return r;
     char *rec = (char *)records;
-    for (int64_t off = 0; off < cnt; off += kChunk) {
-        int64_t m = cnt - off < kChunk ? cnt - off : kChunk;
+    // conversion + DMA of chunk i + 1 into pinned buffer (i + 1) % 2 overlap
+    // the host copy of chunk i out of the other buffer
+    const int64_t nch = (cnt + kPinRecords - 1) / kPinRecords;
+    auto enqueue = [&](int64_t i) -> cudaError_t {
+        const int64_t off = i * kPinRecords, m = cnt - off < kPinRecords ? cnt - off : kPinRecords;
         launch_download_particles(c, kind, c->d_stage, m, off);
-        CK(cudaMemcpyAsync(rec + 144 * off, c->d_stage, (size_t)m * 144, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
+        cudaError_t e = cudaMemcpyAsync(c->h_pin[i & 1], c->d_stage, (size_t)m * 144, cudaMemcpyDeviceToHost,
+                                        c->stream);
+        return e != cudaSuccess ? e : cudaEventRecord(c->pin_ev[i & 1], c->stream);
+    };
+    CK(enqueue(0));
+    for (int64_t i = 0; i < nch; ++i) {
+        if (i + 1 < nch) CK(enqueue(i + 1));
+        CK(cudaEventSynchronize(c->pin_ev[i & 1]));
+        const int64_t off = i * kPinRecords, m = cnt - off < kPinRecords ? cnt - off : kPinRecords;
+        par_memcpy(rec + 144 * off, c->h_pin[i & 1], (size_t)m * 144);
     }
     r = launch_check(c, "pic_download_particles");
     return r ? r : st;

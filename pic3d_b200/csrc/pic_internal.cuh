@@ -169,6 +169,12 @@ struct pic_ctx {
     int *d_list = nullptr;               // compaction index lists
     int64_t list_cap = 0;
     double *d_diag = nullptr;
+    // pinned host staging for particle uploads / downloads: two buffers of
+    // kPinRecords records each, used alternately so that the host copy of
+    // one chunk overlaps the DMA of the other
+    void *h_pin[2] = {nullptr, nullptr};
+    int64_t pin_records = 0;
+    cudaEvent_t pin_ev[2] = {nullptr, nullptr};
     // tiling / sorting
     int tile = 0;                        // tile edge in cells (0: global-memory kernel only)
     int ntile[3] = {0, 0, 0};

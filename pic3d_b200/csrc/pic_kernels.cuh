@@ -42,7 +42,8 @@ void launch_thermal_records(pic_ctx *c, const ThermalArgs &a);
 void launch_push(pic_ctx *c, int kind);
 void launch_push_list(pic_ctx *c, int kind, const int *idx, const unsigned long long *count);
 void launch_remove(pic_ctx *c, int kind);
-void launch_upload_particles(pic_ctx *c, int kind, const void *d_records, int64_t n, int64_t offset);
+void launch_upload_particles(pic_ctx *c, int kind, const void *d_records, int64_t n, int64_t offset,
+                             unsigned long long *check = nullptr);
 void launch_download_particles(pic_ctx *c, int kind, void *d_records, int64_t n, int64_t offset);
 void launch_convert_array(pic_ctx *c, void *dst, const void *src, long long n, int to_device);
 void launch_deposit_one(pic_ctx *c, int kind, const double (&xo)[3], const double (&xn)[3], double qw);

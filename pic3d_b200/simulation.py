@@ -130,7 +130,7 @@ class Simulation:
 
     def download_particles(self, kind: int) -> np.ndarray:
         n = self.num_particles(kind)
-        out = np.zeros(n, dtype=PARTICLE_DTYPE)
+        out = np.empty(n, dtype=PARTICLE_DTYPE)   # every byte is written by the download
         got = ctypes.c_int64()
         self._check(self.lib.pic_download_particles(self.ctx, kind, out.ctypes.data if n else None, n,
                                                     ctypes.byref(got)))

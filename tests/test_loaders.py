@@ -253,3 +253,41 @@ def test_gpu_thermal_generator(precision):
             np.testing.assert_allclose(np.stack([a["px"], a["py"], a["pz"]]),
                                        np.stack([r["px"], r["py"], r["pz"]]), rtol=1e-6, atol=1e-9)
         np.testing.assert_array_equal(a["weight"], r["weight"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_gpu_upload_download_round_trip_over_chunks(precision):
+    """More records than one pinned staging buffer (262,144): download,
+    upload back, download again gives the same records."""
+    from pic3d_b200.simulation import Simulation
+    w = tiny_cases()["periodic_o4"].with_(nx=48, ny=40, nz=36)
+    with Simulation(w, precision=precision) as sim:
+        sim.generate_thermal(0, 4, 1.0, 0.05, 77)    # 276,480 particles
+        a = sim.download_particles(0)
+        assert len(a) == 48 * 40 * 36 * 4
+        sim.upload_particles(0, a)
+        b = sim.download_particles(0)
+    for f in PARTICLE_DTYPE.names:
+        assert np.array_equal(a[f], b[f]), f
+
+
+@pytest.mark.gpu
+def test_gpu_upload_rejects_bad_records():
+    from pic3d_b200 import _lib as L
+    from pic3d_b200.simulation import Simulation
+    w = tiny_cases()["periodic_o2"]
+    good = lattice_ref(w, 8, lambda x, y, z: 1.0, charge=-1.0, mass=1.0)
+    with Simulation(w, precision="fp64") as sim:
+        for field, value in (("charge", 1.0), ("weight", np.nan), ("mass", 2.0)):
+            bad = good.copy()
+            bad[field][len(bad) // 2] = value
+            with pytest.raises(L.PicError) as e:
+                sim.upload_particles(0, bad)
+            assert e.value.code == L.PIC_EINVAL
+            assert sim.num_particles(0) == 0
+        sim.upload_particles(0, good)
+        got = sim.download_particles(0)
+    assert len(got) == len(good)
+    for f in ("id", "x", "y", "z", "px", "weight", "charge", "mass"):
+        assert np.array_equal(np.sort(got[f]), np.sort(good[f])), f
