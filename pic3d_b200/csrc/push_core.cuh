@@ -155,8 +155,9 @@ struct FixedAcc {
     __device__ __forceinline__ bool has_rho() const { return p[3] != nullptr; }
     __device__ __forceinline__ real coef(int c) const { return scale[c]; }
     // q is already scaled.  Rounded to the nearest integer and split into
-    // limbs q = l2*2^40 + l1*2^20 + l0 (FP64) or q = h*2^20 + l0 (FP32), with
-    // l0, l1 in [0, 2^20) and the top limb signed.  FP64 rounds by the
+    // limbs q = l2*2^40 + l1*2^20 + l0 (FP64) or q = h*2^20 + l0 (FP32 current),
+    // with l0, l1 in [0, 2^20) and the top limb signed; FP32 rho (c == 3) is
+    // scaled below 2^19 and added as one signed word.  FP64 rounds by the
     // add-a-magic-constant method (the sum's low mantissa bits are the
     // integer), FP32 by a float-to-int conversion.  Zeros are skipped: a
     // particle at rest (cold plasma) deposits no current.
@@ -168,6 +169,8 @@ struct FixedAcc {
             atomicAdd(a, (unsigned)(qi & 0xFFFFF));
             atomicAdd(a + lstride, (unsigned)((qi >> 20) & 0xFFFFF));
             atomicAdd(a + 2 * lstride, (unsigned)(int)(qi >> 40));
+        } else if (c == 3) {                                               // rho: |q| < 2^19, one word
+            atomicAdd(a, (unsigned)__float2int_rn(q));
         } else {                                                           // |q| < 2^31
             const int qi = __float2int_rn(q);
             atomicAdd(a, (unsigned)qi & 0xFFFFFu);

@@ -347,14 +347,20 @@ struct TileArgs {
     unsigned long long *nstrag;
 };
 
-// CTAs per SM the register allocation must allow: two for FP32 (measured
-// 1.46x faster at 4th order than one CTA with more registers), one for FP64
-// (which spills under the tighter budget)
+// Threads per CTA and CTAs per SM the register allocation must allow.
+// FP32: two CTAs of 256 threads (measured 1.46x faster at 4th order than
+// one CTA with more registers).  FP64: its 143 KB of shared memory allows
+// one CTA per SM; 512 threads at 128 registers (a few spills) measured 12 %
+// faster on the laser workload than 256 at 237 registers, while 384 lost
+// (a tile's 512 particles per species then leave a third of the second
+// round idle).
 template <typename real>
 constexpr int tile_min_blocks() { return sizeof(real) == 4 ? 2 : 1; }
+template <typename real>
+constexpr int tile_threads() { return sizeof(real) == 4 ? 256 : 512; }
 
 template <typename real, int P, bool SPIN>
-__global__ void __launch_bounds__(256, tile_min_blocks<real>()) tile_push_kernel(TileArgs<real> ta) {
+__global__ void __launch_bounds__(tile_threads<real>(), tile_min_blocks<real>()) tile_push_kernel(TileArgs<real> ta) {
     constexpr int H = P / 2;
     constexpr int NL = limbs<real>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -460,7 +466,7 @@ __global__ void __launch_bounds__(256, tile_min_blocks<real>()) tile_push_kernel
         int lz = l / D2, r = l - lz * D2, ly = r / DE, lx = r - ly * DE;
         const unsigned *q = sa + c * NL * DS + lz * dsz + ly * dsy + lx;
         long long tot;
-        if constexpr (NL == 2) tot = ((long long)(int)q[DS] << 20) + (long long)q[0];
+        if constexpr (NL == 2) tot = c >= 3 ? (long long)(int)q[0] : ((long long)(int)q[DS] << 20) + (long long)q[0];
         else tot = ((long long)(int)q[2 * DS] << 40) + ((long long)q[DS] << 20) + (long long)q[0];
         if (tot == 0) continue;
         int x = dO[0] + lx, y = dO[1] + ly, z = dO[2] + lz;
@@ -505,13 +511,22 @@ static void tile_push_t(pic_ctx *c, int mask) {
     for (int k = 0; k < 5; ++k) ta.ring[k] = (real *)c->ring[k];
     for (int k = 0; k < 6; ++k) ta.field[k] = (const real *)c->field[k];
     // one contribution is at most |q w| d/dt (J: the running sum of ds and the
-    // Esirkepov weight are both within [-1, 1]) or |q w| (rho)
+    // Esirkepov weight are both within [-1, 1]) or |q w| smax^3 (rho, smax the
+    // largest shape weight: 3/4 at 2nd order, 115/192 at 4th)
     const double dmax = std::max(c->p.dx, std::max(c->p.dy, c->p.dz));
     const double lim = std::ldexp(1.0, 20 * limbs<real>() - 9);
-    const double bj = 1.01 * qw_max * dmax / c->p.dt, br = 1.01 * qw_max;
+    const double smax = P == 3 ? 0.75 : 115.0 / 192.0;
+    const double bj = 1.01 * qw_max * dmax / c->p.dt, br = 1.01 * qw_max * smax * smax * smax;
+    // FP32 rho is one signed 32-bit word per point: kMaxTileParticles
+    // contributions below 2^19 each cannot overflow.  The resolution, 2^-19
+    // of the largest possible contribution, leaves a point's sum of a few
+    // thousand rounded contributions within about 1e-6 of itself: rho
+    // contributions carry no velocity factor, so (unlike J) they are never
+    // far below their bound
+    const double lim_rho = limbs<real>() == 2 ? std::ldexp(1.0, 19) : lim;
     for (int k = 0; k < 4; ++k) {
         double b = k < 3 ? bj : br;
-        double s = b > 0.0 ? lim / b : 1.0;
+        double s = b > 0.0 ? (k < 3 ? lim : lim_rho) / b : 1.0;
         ta.scale[k] = (real)s;
         ta.inv_scale[k] = 1.0 / (double)ta.scale[k];
     }
@@ -521,7 +536,7 @@ static void tile_push_t(pic_ctx *c, int mask) {
     size_t smem = tile_smem_bytes(c);
     cudaFuncSetAttribute(tile_push_kernel<real, P, SPIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int ntiles = c->ntile[0] * c->ntile[1] * c->ntile[2];
-    tile_push_kernel<real, P, SPIN><<<ntiles, 256, smem, c->stream>>>(ta);
+    tile_push_kernel<real, P, SPIN><<<ntiles, tile_threads<real>(), smem, c->stream>>>(ta);
 }
 
 void launch_tile_push(pic_ctx *c, int mask) {
