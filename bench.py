@@ -1,20 +1,25 @@
 """Benchmark of the PIC3D per-timestep loop on B200.
 
-Workload (default): the laser-in-underdense-plasma configuration —
-256 x 128 x 128 cells, dx = lambda/20, dy = dz = lambda/10, electrons and
-protons at 8 particles per cell each (67,108,864 particles), density
-0.01 n_c on a linear ramp, cold start, a0 = 2 laser from x-min, absorbing
-faces, 4th-order shapes, FP64.  Synthetic seeded inputs of that shape.
-A step is one iteration of the reference's run_main_time_loop over all
-particles and cells.
+Headline workload: the throughput scale-up configuration -- a periodic
+512 x 256 x 256 thermal electron-proton plasma, 8 particles per cell per
+species (536,870,912 particles), u_th = 0.02 c for both species, 2nd-order
+shapes, FP64.  Seeded synthetic inputs of that shape (the device generator
+pic_generate_thermal).  A step is one iteration of the reference's
+run_main_time_loop over all particles and cells.  The same configuration in
+FP32 and at 4th order is timed beside it (`variants`), the FP32 error
+against FP64 is measured per step on the 32^3 thermal plasma (`fp32_error`),
+the laser-in-underdense-plasma configuration is timed after the pulse has
+entered the plasma (`laser`), and the differentiable run gives the adjoint /
+forward time (`adjoint`).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 Prints one JSON line (rank 0).  `value` is device-resident particle-steps/s
 summed over ranks (each rank runs an independent replica: the reference's
 only parallelism is MPI domain decomposition, which this single-GPU path
-does not implement), `e2e` the same metric through the C ABI with host
-buffers, `roofline` the dominant kernel against the measured HBM copy
+does not implement), `e2e` the same metric through the C ABI with the
+particle state read from and written back to host memory inside the timed
+region, `roofline` the dominant kernel against the measured HBM copy
 bandwidth, `cpu_baseline` the reference CPU code on a bounded sample.
 """
 from __future__ import annotations
@@ -59,21 +64,6 @@ def measured_traffic(precision):
         return None
     with open(p) as f:
         return json.load(f)["dram_bytes_per_particle"].get(precision)
-
-
-def workload(name, precision):
-    from pic3d_b200 import workloads as W
-    if name == "laser_underdense":
-        return W.laser_underdense(precision=precision)
-    if name == "laser_underdense_small":
-        return W.laser_underdense(nx=64, ny=32, nz=32, precision=precision)
-    if name == "laser_underdense_medium":
-        return W.laser_underdense(nx=128, ny=64, nz=64, precision=precision)
-    if name == "thermal_scaleup":
-        return W.thermal_scaleup(precision=precision)
-    if name in ("thermal_o2_medium", "thermal_o4_medium"):
-        return W.thermal_scaleup(nx=128, ny=64, nz=64, mem=2 if "o2" in name else 4, precision=precision)
-    raise SystemExit(f"unknown workload {name}")
 
 
 class Clocks:
@@ -123,17 +113,37 @@ class Clocks:
 
 TILE = dict(tile=0, sort_interval=0)
 
+# the throughput scale-up configuration (8 + 8 particles per cell, u_th = 0.02)
+SCALEUP_PPC, SCALEUP_UTH = 8, 0.02
 
-def make_sim(w, precision, particles, device):
+
+def cpu_info():
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "logical_cpus": os.cpu_count()}
+
+
+def thermal_sim(mem, precision, device, seed, nx=512, ny=256, nz=256):
+    """The scale-up plasma generated on the device (seeded Philox)."""
+    from pic3d_b200 import workloads as W
     from pic3d_b200.simulation import Simulation
+    w = W.thermal_scaleup(nx=nx, ny=ny, nz=nz, mem=mem, precision=precision)
     sim = Simulation(w, precision=precision, device=device, **TILE)
     for k in range(2):
-        sim.upload_particles(k, particles[k])
-    return sim
+        sim.generate_thermal(k, SCALEUP_PPC, 1.0, SCALEUP_UTH, seed + k)
+    return w, sim
 
 
 def timed_steps(sim, steps, prof=True):
-    """K steps bracketed by CUDA events on the library's stream."""
+    """K steps bracketed by CUDA events on the library's stream; with
+    prof, per-kernel CUDA-event totals on the same stream."""
     import torch
     stream = torch.cuda.ExternalStream(sim.stream())
     sim.synchronize()
@@ -152,50 +162,250 @@ def timed_steps(sim, steps, prof=True):
     return ms, kern
 
 
-def cpu_baseline(precision_bytes_note=None, target_s=15.0):
-    """Reference CPU code (oracle/_ref) on a bounded sub-box sample of the
-    same per-particle workload (4th order, 8+8 particles per cell, laser
-    parameters), one process, one core.  Falls back to the C port."""
+def count_kernel_launches(sim, steps=1):
+    """Kernels this library launches per step, counted in the CUDA activity
+    trace of torch.profiler (every kernel on the device, whatever stream;
+    the library's kernels live in namespace pic); None if no trace."""
+    try:
+        import torch
+        from torch.profiler import ProfilerActivity, profile
+        sim.synchronize()
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            sim.run_main_time_loop(steps)
+            sim.synchronize()
+        n = sum(1 for e in prof.events()
+                if e.device_type == torch.autograd.DeviceType.CUDA and "pic::" in e.name)
+        return n / steps if n else None
+    except Exception:
+        return None
+
+
+def tile_roofline(kern, npart, ncell, precision, peak, peak_kind, ms_step):
+    """HBM roofline of the tiled push kernel from its CUDA-event launch
+    times: algorithmic bytes per launch / average launch duration."""
+    t = kern.get("tile_push_gather_deposit")
+    if not t or t[1] <= 0:
+        return None
+    avg_ms = t[0] / t[1]
+    per = BYTES_PER_PARTICLE[precision] + GRID_BYTES_PER_CELL[precision] * ncell / max(npart, 1)
+    achieved = per * npart / (avg_ms / 1e3) / 1e9
+    tpp = measured_traffic(precision)
+    return {"bound": "hbm", "kernel": "tile_push_gather_deposit", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind,
+            "traffic": tpp * npart if tpp else None,
+            "traffic_note": ("dram read+write bytes per launch: bytes per particle from an ncu capture of a "
+                             "smaller case of the same workload, times the particles per launch") if tpp else None,
+            "bytes_per_particle": per, "avg_launch_ms": avg_ms, "share_of_step": t[0] / ms_step}
+
+
+def run_case(sim, warmup, steps, clocks=None):
+    sim.initial_push()
+    sim.run_main_time_loop(warmup)
+    sim.synchronize()
+    if clocks:
+        clocks.start()
+    ms, kern = timed_steps(sim, steps, prof=True)
+    clk = clocks.stop() if clocks else None
+    return ms, kern, clk
+
+
+def variants_bench(local, rank, warmup, steps, skip=None):
+    """The scale-up configuration at both orders and precisions (the
+    headline's own case excluded)."""
+    from pic3d_b200.simulation import Simulation  # noqa: F401
+    peak, peak_kind = measured_peaks()
+    out = []
+    for mem, prec in ((2, "fp32"), (4, "fp64"), (4, "fp32")):
+        if skip == (mem, prec):
+            continue
+        w, sim = thermal_sim(mem, prec, local, 97 + 2 * rank)
+        npart = sum(sim.num_particles(k) for k in range(2))
+        ncell = w.nx * w.ny * w.nz
+        ms, kern, _ = run_case(sim, warmup, steps)
+        sim.close()
+        roof = tile_roofline(kern, npart, ncell, prec, peak, peak_kind, ms)
+        out.append({"order": 2 if mem == 2 else 4, "precision": prec, "particles": npart,
+                    "particle_steps_per_s": npart * steps / (ms / 1e3), "ms_per_step": ms / steps,
+                    "cell_updates_per_s": ncell * steps / (ms / 1e3),
+                    "tile_push_ms": roof["avg_launch_ms"] if roof else None,
+                    "tile_push_roofline_frac": roof["frac"] if roof else None,
+                    "kernels": {k: {"ms_total": v[0], "launches": v[1]} for k, v in kern.items()}})
+    return out
+
+
+def fp32_error_bench(local, steps=200, samples=(1, 2, 5, 10, 20, 50, 100, 200)):
+    """The FP32 path against FP64 on the 32^3 thermal plasma (8 electrons
+    per cell, u_th = 0.05, ions a fixed background, 2nd order; the FP64 GPU
+    run equals the FP64 oracle per step to 1e-10): teacher-forced per-step
+    relative L2 error of every field, current and particle array (the FP64
+    state n uploaded into the FP32 context, one step, compared with FP64
+    step n+1), and the free-running error of the two runs side by side with
+    their energies."""
+    from pic3d_b200 import workloads as W
+    from pic3d_b200.simulation import Simulation
+
+    def rel(a, b):
+        nb = float(np.linalg.norm(b))
+        return float(np.linalg.norm(a - b)) / nb if nb > 0 else 0.0
+
+    names = ("ex", "ey", "ez", "bx", "by", "bz", "jx", "jy", "jz", "rho0")
+    out = {"workload": "thermal_periodic_32^3, 8 electrons per cell, u_th 0.05, order 2", "steps": steps,
+           "teacher_forced": {}, "free_running": {}}
+    w = W.thermal_periodic(32, mem=2, steps=steps)
+    parts = W.make_particles(w, seed=1234)
+    s64 = Simulation(w, precision="fp64", device=local, **TILE)
+    s32 = Simulation(w, precision="fp32", device=local, **TILE)
+    t32 = Simulation(w, precision="fp32", device=local, **TILE)
+    for s in (s64, s32):
+        for k in range(2):
+            s.upload_particles(k, parts[k])
+        s.initial_push()
+    for n in range(1, steps + 1):
+        if n in samples:
+            st = s64.state()
+            t32.upload_state(st)
+            t32.step = n - 1
+        s64.run_main_time_loop(1)
+        s32.run_main_time_loop(1)
+        if n in samples:
+            t32.run_main_time_loop(1)
+            a64, a32, f32 = s64.state(), s32.state(), t32.state()
+            d64, d32 = s64.diagnostics(), s32.diagnostics()
+            e64 = d64["field_energy"] + d64["kinetic0"]
+            e32 = d32["field_energy"] + d32["kinetic0"]
+            pa, pb = np.sort(f32["particles"][0], order="id"), np.sort(a64["particles"][0], order="id")
+            mom = rel(np.stack([pa["px"], pa["py"], pa["pz"]]), np.stack([pb["px"], pb["py"], pb["pz"]]))
+            out["teacher_forced"][n] = dict({k: rel(f32[k], a64[k]) for k in names}, momenta=mom)
+            out["free_running"][n] = dict({k: rel(a32[k], a64[k]) for k in ("ex", "ey", "ez", "bx", "by", "bz",
+                                                                             "jx", "jy", "jz")},
+                                          total_energy_fp64=e64, total_energy_fp32=e32,
+                                          energy_rel_diff=abs(e32 - e64) / abs(e64))
+    for s in (s64, s32, t32):
+        s.close()
+    tf = out["teacher_forced"]
+    out["teacher_forced_max"] = max(max(v.values()) for v in tf.values())
+    out["note"] = ("teacher-forced: one FP32 step from the FP64 state, the per-step error the 1e-5 bound applies "
+                   "to; free-running: the two runs diverge as any chaotic plasma does, shown for reference")
+    return out
+
+
+def laser_bench(local, rank, warmup_steps, steps, precision):
+    """The laser-in-underdense-plasma configuration (256x128x128, 4th order,
+    8 + 8 particles per cell, a0 = 2, absorbing), timed after `warmup_steps`
+    steps so that the pulse is inside the plasma and electrons move."""
+    from pic3d_b200 import workloads as W
+    from pic3d_b200.simulation import Simulation
+    w = W.laser_underdense(precision=precision)
+    parts = W.make_particles(w, seed=1234 + rank)
+    sim = Simulation(w, precision=precision, device=local, **TILE)
+    for k in range(2):
+        sim.upload_particles(k, parts[k])
+    del parts
+    npart0 = sum(sim.num_particles(k) for k in range(2))
+    ms, kern, _ = run_case(sim, warmup_steps, steps)
+    npart = sum(sim.num_particles(k) for k in range(2))
+    sim.close()
+    peak, peak_kind = measured_peaks()
+    ncell = w.nx * w.ny * w.nz
+    roof = tile_roofline(kern, npart, ncell, precision, peak, peak_kind, ms)
+    return {"workload": w.name, "precision": precision, "timed_after_step": warmup_steps + 1,
+            "particles_at_start": npart0, "particles_timed": npart,
+            "particle_steps_per_s": npart * steps / (ms / 1e3), "ms_per_step": ms / steps,
+            "tile_push_roofline_frac": roof["frac"] if roof else None,
+            "kernels": {k: {"ms_total": v[0], "launches": v[1]} for k, v in kern.items()}}
+
+
+def e2e_bench(local, steps, mem=2, precision="fp64"):
+    """The headline metric through the C ABI with the particle state in host
+    memory: particles generated on the device and downloaded once (untimed)
+    stand for the caller's host arrays; the timed region uploads them
+    (pic_upload_particles, host -> device), runs the t=0 push and K
+    pic_run_steps(1) calls each followed by a pic_diagnostics read-back, and
+    downloads every particle and field array (device -> host)."""
+    from pic3d_b200.simulation import Simulation
+    w, sim = thermal_sim(mem, precision, local, 4242)
+    host = [sim.download_particles(k) for k in range(2)]
+    sim.close()
+    npart = sum(len(h) for h in host)
+    sim = Simulation(w, precision=precision, device=local, **TILE)
+    sim.synchronize()
+    t0 = time.perf_counter()
+    for k in range(2):
+        sim.upload_particles(k, host[k])
+    h2d = sum(h.nbytes for h in host)
+    sim.initial_push()
+    d2h = 0
+    for _ in range(steps):
+        sim.run_main_time_loop(1)
+        sim.diagnostics()
+        d2h += 8 * 6
+    out = [sim.download_particles(k, host[k]) for k in range(2)]   # back into the caller's arrays
+    flds = {n: sim.download_array(n) for n in ("ex", "ey", "ez", "bx", "by", "bz")}
+    dt = time.perf_counter() - t0
+    d2h += sum(p.nbytes for p in out) + sum(a.nbytes for a in flds.values())
+    sim.close()
+    return {"value": npart * steps / dt, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d / steps,
+            "d2h_bytes_per_step": d2h / steps, "seconds": dt,
+            "note": "pic_upload_particles of 144-byte records from host memory, the t=0 push, K pic_run_steps(1) "
+                    "each followed by a pic_diagnostics read-back, pic_download_particles and pic_download_array "
+                    "of the final state, all inside the timed region"}
+
+
+def scaleup_subbox():
+    """The per-process CPU sample of the scale-up configuration: a 32x16x16
+    sub-box with the same particles per cell, u_th and shape order."""
+    from pic3d_b200 import workloads as W
+    w = W.thermal_scaleup(nx=32, ny=16, nz=16, mem=2, precision="fp64")
+    return w, W.make_particles(w, seed=11)
+
+
+def cpu_baseline(target_s=15.0):
+    """Reference CPU code (oracle/_ref, -O2, and the reference Makefile's
+    -O0) on a bounded sample: the 32x16x16 sub-box of the scale-up
+    configuration, one process on one core.  Falls back to the C port."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle as O
-    from pic3d_b200 import workloads as W
-    w = W.laser_underdense(nx=32, ny=16, nz=16, steps=4)
-    parts = W.make_particles(w, seed=11)
+    w, parts = scaleup_subbox()
     n = sum(len(p) for p in parts)
     if O.have_reference_build():
-        # estimate the per-step cost with a short run, then size the sample
         _, t = O.run_reference(w, parts, 2, timing=True)
         per_step = max(t["loop_seconds"] / 2, 1e-3)
-        steps = int(max(2, min(60, target_s / per_step)))
+        steps = int(max(2, min(100, target_s / per_step)))
         _, t = O.run_reference(w, parts, steps, timing=True)
         rate = t["particles_start"] * steps / t["loop_seconds"]
-        return {"value": rate, "unit": "particle-steps/s", "cores": 1, "kind": "reference",
-                "sample": f"reference src/*.cpp -O2, 32x16x16 sub-box of the laser workload "
-                          f"({n} particles, 4th order), {steps} steps, 1 process"}
+        res = {"value": rate, "unit": "particle-steps/s", "cores": 1, "kind": "reference", "cpu": cpu_info(),
+               "sample": f"reference src/*.cpp -O2, 32x16x16 sub-box of the 512x256x256 thermal configuration "
+                         f"({n} particles, 8+8 per cell, u_th 0.02, 2nd order, FP64), {steps} steps, 1 process"}
+        if os.path.exists(O.REF_BIN_O0):
+            s0 = max(2, steps // 4)
+            _, t0 = O.run_reference(w, parts, s0, timing=True, binary=O.REF_BIN_O0)
+            res["value_O0"] = t0["particles_start"] * s0 / t0["loop_seconds"]
+            res["value_O0_note"] = f"the reference Makefile's -O0 build, {s0} steps, same sample"
+        return res
     o = O.Oracle(w, parts)
     o.initial()
     t0 = time.perf_counter()
     o.step(1)
     per_step = time.perf_counter() - t0
-    steps = int(max(2, min(60, target_s / max(per_step, 1e-3))))
+    steps = int(max(2, min(100, target_s / max(per_step, 1e-3))))
     t0 = time.perf_counter()
     o.run(2, steps)
     dt = time.perf_counter() - t0
-    return {"value": n * steps / dt, "unit": "particle-steps/s", "cores": 1, "kind": "port",
-            "sample": f"C restatement (oracle/pic_oracle.c), 32x16x16 sub-box of the laser workload "
-                      f"({n} particles, 4th order), {steps} steps, 1 process"}
+    return {"value": n * steps / dt, "unit": "particle-steps/s", "cores": 1, "kind": "port", "cpu": cpu_info(),
+            "sample": f"C restatement (oracle/pic_oracle.c), 32x16x16 sub-box of the 512x256x256 thermal "
+                      f"configuration ({n} particles, 2nd order), {steps} steps, 1 process"}
 
 
 def reference_arm(args):
     """--impl reference: the reference's own CPU code on all host cores,
-    as concurrent single-rank processes on equal sub-boxes (the reference
-    has no threads; its parallelism is MPI, absent here)."""
+    as concurrent single-rank processes on equal sub-boxes of the scale-up
+    configuration (the reference has no threads; its parallelism is MPI,
+    absent here)."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle as O
-    from pic3d_b200 import workloads as W
     cores = os.cpu_count() or 1
-    w = W.laser_underdense(nx=32, ny=16, nz=16, steps=args.steps)
-    parts = W.make_particles(w, seed=11)
+    w, parts = scaleup_subbox()
+    w = w.with_(steps=args.steps)
     n = sum(len(p) for p in parts)
     use_ref = O.have_reference_build()
     if not use_ref:
@@ -216,29 +426,28 @@ def reference_arm(args):
             pre = ["taskset", "-c", str(c)] if shutil.which("taskset") else []
             procs.append(subprocess.Popen(pre + cmd, env=env, cwd=tmp, stdout=subprocess.PIPE,
                                           stderr=subprocess.PIPE, text=True))
-        rates, secs = [], []
+        secs = []
         for p in procs:
             out, err = p.communicate()
             line = [l for l in out.splitlines() if l.startswith("{")]
             if p.returncode != 0 or not line:
                 raise RuntimeError(f"reference process failed: {err[-500:]}")
-            t = json.loads(line[-1])
-            secs.append(t["loop_seconds"])
-            rates.append(t["particles_start"] * t["steps"] / t["loop_seconds"])
+            secs.append(json.loads(line[-1])["loop_seconds"])
         total = float(n) * args.steps * cores / max(secs)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     kind = "reference" if use_ref else "port"
-    sample = (f"{cores} concurrent single-rank processes (one per core), each a 32x16x16 sub-box of the laser "
-              f"workload ({n} particles, 4th order, FP64), {args.steps} steps")
+    sample = (f"{cores} concurrent single-rank processes (one per core), each a 32x16x16 sub-box of the "
+              f"512x256x256 thermal configuration ({n} particles, 8+8 per cell, u_th 0.02, 2nd order, FP64), "
+              f"{args.steps} steps")
     line = {"impl": "reference", "metric": "particle-steps/s", "value": total, "unit": "particle-steps/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * max(secs) / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "laser_underdense 256x128x128 (CPU sample: 32x16x16 sub-boxes)", "order": 4,
-                       "particles_per_cell": 16},
+            "config": {"workload": "thermal_scaleup 512x256x256 (CPU sample: 32x16x16 sub-boxes per core)",
+                       "order": 2, "particles_per_cell": 16, "u_th": SCALEUP_UTH, "boundaries": "periodic"},
             "cpu_baseline": {"value": total, "unit": "particle-steps/s", "cores": cores, "kind": kind,
-                             "sample": sample},
+                             "sample": sample, "cpu": cpu_info()},
             "e2e": {"value": total, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -323,60 +532,22 @@ def adjoint_bench(steps=600, short_steps=100):
                     "at the absorbing faces)"}
 
 
-def scaleup_bench(local, steps=3, warmup=3):
-    """Throughput scale-up configuration: periodic 512 x 256 x 256 thermal
-    electron-proton plasma, 8 particles per cell per species (536,870,912
-    particles), u_th = 0.02, 2nd- and 4th-order shapes, FP32 and FP64.
-    Particles come from the device generator (pic_generate_thermal: seeded
-    Philox, no host particle memory); a short timed window per case keeps
-    the default run within minutes (the per-step cost is steady: no laser,
-    uniform plasma)."""
-    from pic3d_b200 import workloads as W
-    from pic3d_b200.simulation import Simulation
-    out = []
-    for mem in (2, 4):
-        for prec in ("fp32", "fp64"):
-            w = W.thermal_scaleup(mem=mem, precision=prec)
-            sim = Simulation(w, precision=prec, device=local, **TILE)
-            for k in range(2):
-                sim.generate_thermal(k, 8, 1.0, 0.02, 97 + k)
-            npart = sum(sim.num_particles(k) for k in range(2))
-            sim.initial_push()
-            sim.run_main_time_loop(warmup)
-            ms, kern = timed_steps(sim, steps, prof=True)
-            sim.close()
-            tile = kern.get("tile_push_gather_deposit", (0.0, 1))
-            avg = tile[0] / max(tile[1], 1)
-            ncell = w.nx * w.ny * w.nz
-            per = BYTES_PER_PARTICLE[prec] + GRID_BYTES_PER_CELL[prec] * ncell / npart
-            peak, _ = measured_peaks()
-            out.append({"order": 2 if mem == 2 else 4, "precision": prec, "particles": npart,
-                        "particle_steps_per_s": npart * steps / (ms / 1e3), "ms_per_step": ms / steps,
-                        "cell_updates_per_s": ncell * steps / (ms / 1e3), "tile_push_ms": avg,
-                        "tile_push_roofline_frac": per * npart / (avg / 1e3) / 1e9 / peak if avg > 0 else None})
-    return {"workload": "thermal_scaleup_512x256x256", "cells": [512, 256, 256], "particles_per_cell": 16,
-            "u_th": 0.02, "steps": steps, "warmup": warmup, "results": out}
-
-
-def field_rel_err(a: dict, b: dict):
-    num = sum(float(np.sum((a[n] - b[n]) ** 2)) for n in ("ex", "ey", "ez", "bx", "by", "bz"))
-    den = sum(float(np.sum(b[n] ** 2)) for n in ("ex", "ey", "ez", "bx", "by", "bz"))
-    return (num / den) ** 0.5 if den > 0 else 0.0
-
-
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="laser_underdense")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--order", type=int, default=2, choices=[2, 4], help="headline shape order")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"], help="headline precision")
+    ap.add_argument("--cells", default="512,256,256", help="headline grid (smaller grids for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--no-fp32-error", action="store_true")
+    ap.add_argument("--no-laser", action="store_true")
+    ap.add_argument("--laser-warmup", type=int, default=600)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
-    ap.add_argument("--no-scaleup", action="store_true")
     ap.add_argument("--adjoint-steps", type=int, default=600)
     ap.add_argument("--tile", type=int, default=0, help="shared-memory tile edge (0 default, -1 global kernel)")
     ap.add_argument("--sort-interval", type=int, default=0)
@@ -401,23 +572,14 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    from pic3d_b200 import workloads as W
-    w = workload(args.workload, args.precision)
-    parts = W.make_particles(w, seed=1234 + rank)
-    npart = sum(len(p) for p in parts)
+    nx, ny, nz = (int(v) for v in args.cells.split(","))
+    mem, prec = (2 if args.order == 2 else 4), args.precision
+    w, sim = thermal_sim(mem, prec, local, 97 + 2 * rank, nx, ny, nz)
+    npart = sum(sim.num_particles(k) for k in range(2))
     ncell = w.nx * w.ny * w.nz
-
-    sim = make_sim(w, args.precision, parts, local)
     sim.initial_push()
     sim.run_main_time_loop(args.warmup)
-    sim.synchronize()
-    # count kernel launches per step (profiling pass, untimed)
-    sim.profile(True)
-    sim.profile_reset()
-    sim.run_main_time_loop(1)
-    launches_per_step = sum(v[1] for v in sim.profile_read().values())
-    sim.profile(False)
-
+    launches_per_step = count_kernel_launches(sim, 4)
     clocks = Clocks(local)
     if dist:
         dist.barrier()
@@ -425,100 +587,42 @@ def main():
     clocks.start()
     ms, kern = timed_steps(sim, args.steps, prof=True)
     clk = clocks.stop()
+    sim.close()
     from pic3d_b200.replicas import combine
     ms, npart_all, value = combine(ms, npart, args.steps, dist, device="cuda")
-
-    # dominant kernel roofline
     peak, peak_kind = measured_peaks()
-    top = max(kern.items(), key=lambda kv: kv[1][0]) if kern else ("", (0.0, 0))
-    prec = args.precision
-    per_particle = BYTES_PER_PARTICLE[prec] + GRID_BYTES_PER_CELL[prec] * ncell / max(npart, 1)
-    roof = None
-    if top[0] in ("push_gather_deposit", "tile_push_gather_deposit") and top[1][1] > 0:
-        avg_ms = top[1][0] / top[1][1]
-        # the global kernel runs once per species, the tiled one once for both
-        per_launch = npart / 2.0 if top[0] == "push_gather_deposit" else float(npart)
-        bytes_per_launch = per_particle * per_launch
-        achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
-        tpp = measured_traffic(prec) if top[0] == "tile_push_gather_deposit" else None
-        roof = {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_kind": peak_kind,
-                "traffic": tpp * per_launch if tpp else None,
-                "traffic_note": "dram read+write bytes per launch, scaled by particles from an ncu capture of "
-                                "128x64x64 cells" if tpp else None,
-                "bytes_per_particle": per_particle, "avg_launch_ms": avg_ms,
-                "share_of_step": top[1][0] / ms}
+    roof = tile_roofline(kern, npart, ncell, prec, peak, peak_kind, ms)
     kernels = {k: {"ms_total": v[0], "launches": v[1]} for k, v in kern.items()}
 
     extra = {}
-    # FP32 path on the same inputs: throughput and error against FP64
-    if not args.no_fp32 and prec == "fp64":
-        st64 = {n: sim.download_array(n) for n in ("ex", "ey", "ez", "bx", "by", "bz")}
-        sim.close()
-        sim32 = make_sim(w, "fp32", parts, local)
-        sim32.initial_push()
-        sim32.run_main_time_loop(args.warmup + 1)
-        ms32, kern32 = timed_steps(sim32, args.steps, prof=True)
-        st32 = {n: sim32.download_array(n) for n in ("ex", "ey", "ez", "bx", "by", "bz")}
-        err = field_rel_err(st32, st64)
-        kname = "tile_push_gather_deposit" if "tile_push_gather_deposit" in kern32 else "push_gather_deposit"
-        t32 = kern32.get(kname, (0.0, 1))
-        avg32 = t32[0] / max(t32[1], 1)
-        pp32 = BYTES_PER_PARTICLE["fp32"] + GRID_BYTES_PER_CELL["fp32"] * ncell / max(npart, 1)
-        per_launch32 = npart / 2.0 if kname == "push_gather_deposit" else float(npart)
-        ach32 = pp32 * per_launch32 / (avg32 / 1e3) / 1e9 if avg32 > 0 else None
-        extra["fp32"] = {"value": npart_all * args.steps / (ms32 / 1e3), "ms_per_step": ms32 / args.steps,
-                         "field_rel_l2_vs_fp64": err,
-                         "error_note": f"E,B after {args.warmup + 1 + args.steps} steps vs the FP64 GPU run "
-                                       "(itself within 1e-10/step of the FP64 oracle)",
-                         "roofline": {"kernel": kname, "achieved": ach32, "peak": peak,
-                                      "unit": "GB/s", "frac": (ach32 / peak) if ach32 else None}}
-        sim32.close()
-    else:
-        sim.close()
-
-    # end to end through the C ABI with host buffers
+    if not args.no_variants:
+        try:
+            extra["variants"] = variants_bench(local, rank, args.warmup, args.steps, skip=(mem, prec))
+        except Exception as e:
+            extra["variants"] = {"error": str(e)[:300]}
+    if rank == 0 and not args.no_fp32_error:
+        try:
+            extra["fp32_error"] = fp32_error_bench(local)
+        except Exception as e:
+            extra["fp32_error"] = {"error": str(e)[:300]}
+    if not args.no_laser:
+        try:
+            extra["laser"] = [laser_bench(local, rank, args.laser_warmup, args.steps, p) for p in ("fp64", "fp32")]
+        except Exception as e:
+            extra["laser"] = {"error": str(e)[:300]}
     e2e = None
     if not args.no_e2e:
-        from pic3d_b200.simulation import Simulation
-        torch.cuda.synchronize()
-        host_fields = {n: np.zeros((w.nz + 2 * w.mem, w.ny + 2 * w.mem, w.nx + 2 * w.mem)) for n in
-                       ("ex", "ey", "ez", "bx", "by", "bz")}
-        simE = Simulation(w, precision=prec, device=local, **TILE)
-        t0 = time.perf_counter()
-        for n, a in host_fields.items():
-            simE.upload_array(n, a)
-        for k in range(2):
-            simE.upload_particles(k, parts[k])
-        h2d = sum(a.nbytes for a in host_fields.values()) + sum(p.nbytes for p in parts)
-        simE.initial_push()
-        d2h = 0
-        for s in range(args.steps):
-            simE.run_main_time_loop(1)
-            simE.diagnostics()
-            d2h += 8 * 6
-        out = [simE.download_particles(k) for k in range(2)]
-        flds = {n: simE.download_array(n) for n in ("ex", "ey", "ez", "bx", "by", "bz")}
-        dt = time.perf_counter() - t0
-        d2h += sum(p.nbytes for p in out) + sum(a.nbytes for a in flds.values())
-        simE.close()
-        e2e = {"value": npart * args.steps / dt * (world if world > 1 else 1), "unit": "particle-steps/s",
-               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-               "note": "pic_upload_* of the initial state from host memory, the t=0 push, K pic_run_steps(1) "
-                       "each followed by a pic_diagnostics read-back, pic_download_* of the final state"}
-
-    if not args.no_scaleup:
         try:
-            extra["scaleup"] = scaleup_bench(local)
+            e2e = e2e_bench(local, args.steps, mem, prec)
+            if world > 1:
+                e2e["value"] *= world
         except Exception as e:
-            extra["scaleup"] = {"error": str(e)[:300]}
-
+            e2e = {"error": str(e)[:300]}
     if rank == 0 and not args.no_adjoint:
         try:
             extra["adjoint"] = adjoint_bench(args.adjoint_steps)
         except Exception as e:
             extra["adjoint"] = {"error": str(e)[:300]}
-
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         try:
@@ -527,17 +631,18 @@ def main():
             cpu = {"value": None, "error": str(e)[:200]}
 
     if rank == 0:
+        state_gb = npart * (BYTES_PER_PARTICLE[prec] / 2) / 1e9
         line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if prec == "fp64" else "f32", "data": "synthetic",
                 "config": {"workload": w.name, "cells": [w.nx, w.ny, w.nz], "order": w.order,
-                           "tile": args.tile, "sort_interval": args.sort_interval,
-                           "particles": npart, "particles_per_cell": sum(w.ppc), "boundaries": "periodic" if all(w.period) else "absorbing+laser",
-                           "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (particle state "
-                                                                   f"{npart * BYTES_PER_PARTICLE[prec] / 1e9:.1f} GB)"},
+                           "particles": npart, "particles_per_cell": 2 * SCALEUP_PPC, "u_th": SCALEUP_UTH,
+                           "boundaries": "periodic", "tile": args.tile, "sort_interval": args.sort_interval,
+                           "parallelism": f"replicas{world}",
+                           "l2": f"inputs larger than L2 (particle state {state_gb:.1f} GB)"},
                 "cell_updates_per_s": ncell * world * args.steps / (ms / 1e3),
-                "gpu_launches": int(launches_per_step * args.steps),
+                "gpu_launches": int(launches_per_step * args.steps) if launches_per_step else None,
                 "roofline": roof, "kernels": kernels, "clocks": clk, "e2e": e2e, "cpu_baseline": cpu}
         line.update(extra)
         print(json.dumps(line), flush=True)

@@ -96,8 +96,11 @@ int pic_download_array(pic_ctx *ctx, int which, double *host);
 
 /* Particles of species `kind` as reference 144-byte records (particle.h:9-29).
  * Upload replaces the species' particles; every record must carry the
- * species' charge and mass and a finite weight (checked on the device while
- * converting: a bad record returns PIC_EINVAL and leaves the species empty).
+ * species' charge and mass and a finite weight (PIC_EINVAL otherwise), a
+ * finite position and momentum (PIC_ENAN) and, in an FP32 context, a
+ * position whose cell lies in -1 .. n along every absorbing axis (PIC_EOOB:
+ * the packed cell index cannot hold it).  The checks run on the device while
+ * converting; a bad record leaves the species empty.
  * Both directions stream through pinned host buffers owned by the context,
  * the host copy of one chunk overlapping the transfer of the next; the
  * caller's buffer may be ordinary (pageable) memory.  Download writes at most `cap` records and the

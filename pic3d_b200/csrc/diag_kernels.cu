@@ -46,12 +46,13 @@ __global__ void field_diag_kernel(Geom g, const real *ex, const real *ey, const 
         double div = ((double)ex[c] - (double)ex[c - 1]) * idx + ((double)ey[c] - (double)ey[c - g.f[0]]) * idy +
                      ((double)ez[c] - (double)ez[c - g.fxy]) * idz;
         double res = fabs(div - rho0 - rho1);
-        gmax = res > gmax ? res : gmax;
+        gmax = (res != res || res > gmax) ? res : gmax;   // a NaN residual wins and stays
     }
     block_add(0.5 * e * dV, out + 0);
     block_add(q0 * dV, out + 3);
     block_add(q1 * dV, out + 4);
-    // max of non-negative doubles through their ordered bit patterns
+    // max of non-negative doubles through their ordered bit patterns (a
+    // positive NaN orders above every finite value and +inf)
     atomicMax((unsigned long long *)(out + 5), (unsigned long long)__double_as_longlong(gmax));
 }
 

@@ -25,10 +25,14 @@ Geom make_geom(const PicParams &p) {
         g.r[d] = g.f[d] + 2;
         g.per[d] = p.rank_period[d] ? 1 : 0;
     }
-    g.fxy = g.f[0] * g.f[1];
-    g.rxy = g.r[0] * g.r[1];
-    g.fsz = (long long)g.fxy * g.f[2];
-    g.rsz = (long long)g.rxy * g.r[2];
+    // sizes in 64 bits from the extents, so that a caller's check of rsz
+    // against the 32-bit index range is meaningful even where the plane
+    // strides (int) would overflow; the strides are only used once that
+    // check has passed
+    g.fsz = (long long)g.f[0] * g.f[1] * g.f[2];
+    g.rsz = (long long)g.r[0] * g.r[1] * g.r[2];
+    g.fxy = (int)((long long)g.f[0] * g.f[1]);
+    g.rxy = (int)((long long)g.r[0] * g.r[1]);
     return g;
 }
 

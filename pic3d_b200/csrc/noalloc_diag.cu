@@ -62,6 +62,10 @@ int scratch_for_current_device(double **out) {
 
 }  // namespace
 
+// largest of two residuals with NaN winning (fmax and a plain compare would
+// drop a NaN residual and report a finite Gauss error for a NaN field)
+__device__ __forceinline__ double nan_max(double a, double b) { return (a != a || a > b) ? a : b; }
+
 // one CTA per physical z plane: partial sums in a fixed tree order
 __global__ void __launch_bounds__(256) noalloc_plane_kernel(Geom g, const double *__restrict__ ex,
                                                             const double *__restrict__ ey,
@@ -86,7 +90,7 @@ __global__ void __launch_bounds__(256) noalloc_plane_kernel(Geom g, const double
         q1 += s1;
         double div = (ex[c] - ex[c - 1]) * idx + (ey[c] - ey[c - g.f[0]]) * idy + (ez[c] - ez[c - g.fxy]) * idz;
         double res = fabs(div - s0 - s1);
-        gmax = res > gmax ? res : gmax;
+        gmax = nan_max(res, gmax);
     }
     red[0][threadIdx.x] = e;
     red[1][threadIdx.x] = q0;
@@ -98,7 +102,7 @@ __global__ void __launch_bounds__(256) noalloc_plane_kernel(Geom g, const double
             red[0][threadIdx.x] += red[0][threadIdx.x + s];
             red[1][threadIdx.x] += red[1][threadIdx.x + s];
             red[2][threadIdx.x] += red[2][threadIdx.x + s];
-            red[3][threadIdx.x] = fmax(red[3][threadIdx.x], red[3][threadIdx.x + s]);
+            red[3][threadIdx.x] = nan_max(red[3][threadIdx.x], red[3][threadIdx.x + s]);
         }
         __syncthreads();
     }
@@ -120,7 +124,7 @@ __global__ void noalloc_planes_sum_kernel(const double *partials, int nz, double
         e += partials[4 * k + 0];
         q0 += partials[4 * k + 1];
         q1 += partials[4 * k + 2];
-        gmax = fmax(gmax, partials[4 * k + 3]);
+        gmax = nan_max(partials[4 * k + 3], gmax);
     }
     out[0] = 0.5 * e * dV;
     out[1] = q0 * dV;
@@ -144,14 +148,32 @@ extern "C" int pic_field_diagnostics_noalloc(const PicParams *p, const double *e
                      p->local_zcells, PIC_NOALLOC_MAX_PLANES);
         return PIC_EINVAL;
     }
+    if (p->local_xcells > (1 << 20) || p->local_ycells > (1 << 20)) return PIC_EINVAL;
     const Geom g = make_geom(*p);
     if (g.rsz >= (1ll << 31)) return PIC_EINVAL;
     double *partials = nullptr;
     int r = scratch_for_current_device(&partials);
     if (r != PIC_OK) return r;
+    // An error already pending on this thread belongs to earlier work, not to
+    // these launches: report it without consuming it and launch nothing.
+    cudaError_t before = cudaPeekAtLastError();
+    if (before != cudaSuccess) {
+        std::fprintf(stderr, "pic_field_diagnostics_noalloc: CUDA error pending from earlier work: %s\n",
+                     cudaGetErrorString(before));
+        return PIC_ECUDA;
+    }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     noalloc_plane_kernel<<<g.n[2], 256, 0, s>>>(g, ex, ey, ez, bx, by, bz, rho0, rho1, 1.0 / p->dx, 1.0 / p->dy,
                                                  1.0 / p->dz, partials);
-    noalloc_planes_sum_kernel<<<1, 32, 0, s>>>(partials, g.n[2], p->dx * p->dy * p->dz, out);
-    return cudaGetLastError() == cudaSuccess ? PIC_OK : PIC_ECUDA;
+    cudaError_t e = cudaPeekAtLastError();
+    if (e == cudaSuccess) {
+        noalloc_planes_sum_kernel<<<1, 32, 0, s>>>(partials, g.n[2], p->dx * p->dy * p->dz, out);
+        e = cudaPeekAtLastError();
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();   // this launch's own error: consumed here, reported by the status
+        std::fprintf(stderr, "pic_field_diagnostics_noalloc: launch failed: %s\n", cudaGetErrorString(e));
+        return PIC_ECUDA;
+    }
+    return PIC_OK;
 }

@@ -273,8 +273,9 @@ struct ConvArgs {
     int *id;
     double charge, mass;
     // upload checks (null: none): check[0] |= 1 charge/mass differ from the
-    // species', 2 non-finite weight, 4 non-zero spin; check[1] = max |weight|
-    // as the bits of a non-negative double
+    // species', 2 non-finite weight, 4 non-zero spin, 8 non-finite position
+    // or momentum, 16 (FP32) a position whose cell the packed index cannot
+    // hold; check[1] = max |weight| as the bits of a non-negative double
     unsigned long long *check;
 };
 
@@ -309,6 +310,20 @@ __global__ void records_to_soa_kernel(ConvArgs a) {
             if (!isfinite(q.weight)) f |= 2ull;
             else wb = (unsigned long long)__double_as_longlong(fabs(q.weight));
             if (q.sx != 0.0 || q.sy != 0.0 || q.sz != 0.0) f |= 4ull;
+            const double v[6] = {q.x, q.y, q.z, q.px, q.py, q.pz};
+            bool fin = true;
+#pragma unroll
+            for (int d = 0; d < 6; ++d) fin = fin && isfinite(v[d]);
+            if (!fin) f |= 8ull;
+            if (fin && a.fp32) {
+                // the packed FP32 cell holds -1 .. n per axis (after the
+                // periodic wrap): a position beyond cannot be stored
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const double fl = floor(v[d]);
+                    if (!a.g.per[d] && (fl < -1.0 || fl > (double)a.g.n[d])) f |= 16ull;
+                }
+            }
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -582,7 +597,13 @@ __global__ void deposit_one_kernel(PushArgs<real> a, double xo, double yo, doubl
     View<const real> fv[6];
     GlobalAcc<real> acc;
     global_views(a, fv, acc);
-    deposit<real, P>(acc, a.d_dt, i1, d0, i2, d1, (real)qw);
+    Axis1D<real, P> ax[3];
+    bool moved = false;
+    for (int d = 0; d < 3; ++d) {
+        axis_from_offsets<real, P>(i1[d], d0[d], i2[d], d1[d], ax[d]);
+        moved = moved || i1[d] != i2[d] || d0[d] != d1[d];
+    }
+    deposit<real, P>(acc, a.d_dt, ax, moved, (real)qw);
 }
 
 void launch_deposit_one(pic_ctx *c, int kind, const double (&xo)[3], const double (&xn)[3], double qw) {

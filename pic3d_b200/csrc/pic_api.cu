@@ -368,6 +368,8 @@ int pic_create(const PicParams *pp, int device, pic_ctx **out) {
         if (!(p.dt > 0.0) || !(p.dt < d[k])) return bad("dt must satisfy 0 < dt < min(dx,dy,dz) (a particle moves less than a cell per step)");
     }
     if (!(p.mass[0] > 0.0) || !(p.mass[1] > 0.0)) return bad("species masses must be positive");
+    for (int k = 0; k < 3; ++k)
+        if (n[k] < 1 || n[k] > (1 << 20)) return bad("cell counts must lie in [1, 2^20]");
     c->g = make_geom(p);
     if (c->g.rsz >= (1ll << 31)) return bad("grid too large for 32-bit buffer indexing");
     c->fp32 = p.precision == 32;
@@ -545,12 +547,15 @@ int pic_upload_particles(pic_ctx *c, int kind, const void *records, int64_t n) {
     unsigned long long hc[2] = {0, 0};
     CK(cudaMemcpyAsync(hc, chk, sizeof(hc), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    if (hc[0] & 3ull) {
+    if (hc[0] & 27ull) {
         // a bad record leaves the species empty
         r = end_fill(c, kind, 0, "pic_upload_particles");
         if (r) return r;
-        return fail(c, PIC_EINVAL, (hc[0] & 1ull) ? "particle record charge/mass differs from the species parameters"
-                                                 : "non-finite particle weight");
+        if (hc[0] & 1ull) return fail(c, PIC_EINVAL, "particle record charge/mass differs from the species parameters");
+        if (hc[0] & 2ull) return fail(c, PIC_EINVAL, "non-finite particle weight");
+        if (hc[0] & 8ull) return fail(c, PIC_ENAN, "non-finite particle position or momentum");
+        return fail(c, PIC_EOOB, "particle position beyond the cells an FP32 context can store (-1 .. n on an "
+                                 "absorbing axis)");
     }
     Species &s = c->sp[kind];
     s.spin_nonzero = (hc[0] & 4ull) != 0;
@@ -774,7 +779,8 @@ int pic_update_fields_second(pic_ctx *c) {
 int pic_clear_currents(pic_ctx *c) {
     if (!c) return PIC_EINVAL;
     prof_begin(c, "clear_currents");
-    for (int k = 0; k < 5; ++k) CK(cudaMemsetAsync(c->ring[k], 0, (size_t)c->g.rsz * real_size(c), c->stream));
+    const int n = c->rho_skip ? 3 : 5;
+    for (int k = 0; k < n; ++k) CK(cudaMemsetAsync(c->ring[k], 0, (size_t)c->g.rsz * real_size(c), c->stream));
     prof_end(c);
     return PIC_OK;
 }
@@ -808,7 +814,7 @@ int pic_exchange_particles(pic_ctx *c, int kind) {
 
 int pic_exchange_currents(pic_ctx *c) {
     if (!c) return PIC_EINVAL;
-    launch_fold_currents(c);
+    launch_fold_currents(c, c->rho_skip ? 7u : 31u);
     return launch_check(c, "exchange_currents");
 }
 
@@ -886,21 +892,31 @@ int pic_initial_push(pic_ctx *c) {
     return pic_exchange_particles(c, 1);
 }
 
+// One iteration of run_main_time_loop.  rho (a diagnostic: it never feeds
+// the fields) is cleared, deposited and folded only when the step's rho can
+// be observed, i.e. on the last step of a pic_run_steps call.
+static int run_one_step(pic_ctx *c, bool rho_observed) {
+    c->step += 1;
+    c->rho_skip = !rho_observed && !c->p.adjoint;
+    int r;
+    if ((r = pic_radiating_boundary(c, 1, 0, c->step))) return r;
+    if ((r = pic_update_fields_first(c))) return r;
+    if ((r = pic_clear_currents(c))) return r;
+    adjoint_record_hook(c);
+    if ((r = push_both(c))) return r;
+    if ((r = pic_exchange_particles(c, 0))) return r;
+    if ((r = pic_exchange_particles(c, 1))) return r;
+    if ((r = pic_exchange_currents(c))) return r;
+    return pic_update_fields_second(c);
+}
+
 int pic_run_steps(pic_ctx *c, int nsteps) {
     if (!c || nsteps < 0) return PIC_EINVAL;
     cudaSetDevice(c->device);
     for (int t = 0; t < nsteps; ++t) {
-        c->step += 1;
-        int r;
-        if ((r = pic_radiating_boundary(c, 1, 0, c->step))) return r;
-        if ((r = pic_update_fields_first(c))) return r;
-        if ((r = pic_clear_currents(c))) return r;
-        adjoint_record_hook(c);
-        if ((r = push_both(c))) return r;
-        if ((r = pic_exchange_particles(c, 0))) return r;
-        if ((r = pic_exchange_particles(c, 1))) return r;
-        if ((r = pic_exchange_currents(c))) return r;
-        if ((r = pic_update_fields_second(c))) return r;
+        int r = run_one_step(c, t + 1 == nsteps);
+        c->rho_skip = false;
+        if (r) return r;
     }
     return PIC_OK;
 }

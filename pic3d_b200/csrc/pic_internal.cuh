@@ -183,6 +183,10 @@ struct pic_ctx {
     unsigned *d_blocksums = nullptr;
     unsigned long long *d_nstrag = nullptr;   // straggler counts, one per species
     int sort_interval = 4;
+    // rho is observable only between ABI calls: the intermediate steps of
+    // one pic_run_steps call neither clear, deposit nor fold it (set while
+    // such a step runs; never in adjoint mode, whose checkpoints copy rho)
+    bool rho_skip = false;
     int steps_since_sort = 0;
     int step = 0;
     std::string err;

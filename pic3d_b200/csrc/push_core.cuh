@@ -101,27 +101,112 @@ __device__ __forceinline__ real gather(const View<const real> &v, int i0, int j0
     return acc;
 }
 
-// 1D pieces of the Esirkepov weights over the union span of the old and new
-// supports (src/particle.cpp:403-419): s0 = old shape, ds = new - old,
-// zero outside each support.  |i2 - i1| <= 1 (checked by the caller).
-// The weights come in FP64 whatever the working precision: ds is a
-// difference of nearly equal weights for a slow particle, and forming it in
-// FP64 keeps the FP32 path's current accurate to FP32 rounding.
+// One axis of a particle's Esirkepov move (src/particle.cpp:403-419): the
+// union span of the old and new supports starts at buffer index `base` and
+// has `len` points (P, or P + 1 when the primal index changed; |i2 - i1| <= 1
+// is checked by the caller); s0 = old shape, ds = new - old, both zero
+// outside their supports; w1 = new shape on i2 - H .. i2 + H (rho).
 template <typename real, int P>
-__device__ __forceinline__ void span1d(int i1, const double (&w0)[P], int i2, const double (&w1)[P], int &base,
-                                       int &len, real (&s0)[P + 1], real (&ds)[P + 1]) {
+struct Axis1D {
+    int base, len, i2;
+    real s0[P + 1], ds[P + 1], w1[P];
+};
+
+// From the old and new primal offsets in FP64 (FP64 positions, and the
+// single-record deposit of either precision): both weight sets in FP64 and
+// ds as their difference, as the reference forms it.
+template <typename real, int P>
+__device__ __forceinline__ void axis_from_offsets(int i1, double d0, int i2, double d1, Axis1D<real, P> &ax) {
     constexpr int H = P / 2;
+    double w0[P], w1[P];
+    shape_weights(d0, w0);
+    shape_weights(d1, w1);
     const int lo = min(i1, i2);
-    base = lo - H;
-    len = P + abs(i2 - i1);
+    ax.base = lo - H;
+    ax.len = P + abs(i2 - i1);
+    ax.i2 = i2;
     const bool o0 = i1 != lo, o1 = i2 != lo;
 #pragma unroll
     for (int a = 0; a <= P; ++a) {
         double v0 = o0 ? (a >= 1 ? w0[a - 1] : 0.0) : (a < P ? w0[a] : 0.0);
         double v1 = o1 ? (a >= 1 ? w1[a - 1] : 0.0) : (a < P ? w1[a] : 0.0);
-        s0[a] = (real)v0;
-        ds[a] = (real)(v1 - v0);
+        ax.s0[a] = (real)v0;
+        ax.ds[a] = (real)(v1 - v0);
     }
+#pragma unroll
+    for (int q = 0; q < P; ++q) ax.w1[q] = (real)w1[q];
+}
+
+// Change of the shape weights over a move by e that stays on one polynomial
+// piece: dw[k] = w_k(d + e) - w_k(d), formed without subtracting weights.
+// Every term carries a factor e, so a slow particle's differences keep full
+// FP32 relative accuracy.  The outer weights are binomial expansions of
+// their single powers; the inner ones follow from the two identities every
+// B-spline shape satisfies, sum_k w_k = 1 and sum_k k w_k = d (centred k),
+// which give sum_k dw_k = 0 and sum_k k dw_k = e.
+__device__ __forceinline__ void shape_diff(float d, float e, float (&dw)[3]) {
+    const float a = 0.5f - d, b = 0.5f + d;
+    dw[0] = 0.5f * e * (e - 2.0f * a);
+    dw[2] = 0.5f * e * (2.0f * b + e);
+    dw[1] = -(dw[0] + dw[2]);
+}
+
+__device__ __forceinline__ float quartic_step(float x, float e) {   // (x + e)^4 - x^4
+    return e * (4.0f * x * x * x + e * (6.0f * x * x + e * (4.0f * x + e)));
+}
+
+__device__ __forceinline__ void shape_diff(float d, float e, float (&dw)[5]) {
+    dw[0] = quartic_step(d - 0.5f, e) * (1.0f / 24.0f);
+    dw[4] = quartic_step(d + 0.5f, e) * (1.0f / 24.0f);
+    dw[2] = 0.25f * quartic_step(d, e) - 0.625f * e * (2.0f * d + e);
+    const float sum = dw[0] + dw[2] + dw[4];             // = -(dw1 + dw3)
+    const float mom = e + 2.0f * dw[0] - 2.0f * dw[4];   // =   dw3 - dw1
+    dw[1] = -0.5f * (sum + mom);
+    dw[3] = 0.5f * (mom - sum);
+}
+
+// FP32: old primal index i1 and offset d0 in [-1/2, 1/2), move e (cells),
+// new primal index i2 (from the stored new position).  A move that crosses
+// the knot between two primal indices (offset 1/2) is split there: the old
+// support's change up to the knot plus the new support's change from it.
+template <int P>
+__device__ __forceinline__ void axis_from_move(int i1, float d0, float e, int i2, Axis1D<float, P> &ax) {
+    constexpr int H = P / 2;
+    float w0[P];
+    shape_weights(d0, w0);
+    ax.i2 = i2;
+    if (i2 == i1) {
+        float dw[P];
+        shape_diff(d0, e, dw);
+        ax.base = i1 - H;
+        ax.len = P;
+#pragma unroll
+        for (int a = 0; a < P; ++a) {
+            ax.s0[a] = w0[a];
+            ax.ds[a] = dw[a];
+        }
+        ax.s0[P] = 0.0f;
+        ax.ds[P] = 0.0f;
+        shape_weights(d0 + e, ax.w1);
+        return;
+    }
+    const bool up = i2 > i1;
+    const float t0 = (up ? 0.5f : -0.5f) - d0;   // old offset to the knot
+    const float t1 = e - t0;                        // knot to the new position
+    float dold[P], dnew[P];
+    shape_diff(d0, t0, dold);
+    shape_diff(up ? -0.5f : 0.5f, t1, dnew);
+    ax.base = min(i1, i2) - H;
+    ax.len = P + 1;
+#pragma unroll
+    for (int a = 0; a <= P; ++a) {
+        // lower support at a = 0 .. P-1, upper at a = 1 .. P
+        const float lo_o = a < P ? (up ? dold[a] : dnew[a]) : 0.0f;
+        const float hi_o = a >= 1 ? (up ? dnew[a - 1] : dold[a - 1]) : 0.0f;
+        ax.ds[a] = lo_o + hi_o;
+        ax.s0[a] = up ? (a < P ? w0[a] : 0.0f) : (a >= 1 ? w0[a - 1] : 0.0f);
+    }
+    shape_weights((up ? -0.5f : 0.5f) + t1, ax.w1);
 }
 
 __device__ __forceinline__ void atomic_add(double *p, double v) { atomicAdd(p, v); }
@@ -155,9 +240,8 @@ struct FixedAcc {
     __device__ __forceinline__ bool has_rho() const { return p[3] != nullptr; }
     __device__ __forceinline__ real coef(int c) const { return scale[c]; }
     // q is already scaled.  Rounded to the nearest integer and split into
-    // limbs q = l2*2^40 + l1*2^20 + l0 (FP64) or q = h*2^20 + l0 (FP32 current),
-    // with l0, l1 in [0, 2^20) and the top limb signed; FP32 rho (c == 3) is
-    // scaled below 2^19 and added as one signed word.  FP64 rounds by the
+    // limbs q = l2*2^40 + l1*2^20 + l0 (FP64) or q = h*2^20 + l0 (FP32),
+    // with l0, l1 in [0, 2^20) and the top limb signed.  FP64 rounds by the
     // add-a-magic-constant method (the sum's low mantissa bits are the
     // integer), FP32 by a float-to-int conversion.  Zeros are skipped: a
     // particle at rest (cold plasma) deposits no current.
@@ -169,8 +253,6 @@ struct FixedAcc {
             atomicAdd(a, (unsigned)(qi & 0xFFFFF));
             atomicAdd(a + lstride, (unsigned)((qi >> 20) & 0xFFFFF));
             atomicAdd(a + 2 * lstride, (unsigned)(int)(qi >> 40));
-        } else if (c == 3) {                                               // rho: |q| < 2^19, one word
-            atomicAdd(a, (unsigned)__float2int_rn(q));
         } else {                                                           // |q| < 2^31
             const int qi = __float2int_rn(q);
             atomicAdd(a, (unsigned)qi & 0xFFFFFu);
@@ -199,25 +281,22 @@ __device__ __forceinline__ void mid_loop(int len, const real (&s0)[P + 1], const
     }
 }
 
-// Esirkepov deposit (src/particle.cpp:427-500) and rho (:503-514).  The
-// last point of each running sum (the sum of all ds, zero up to rounding)
-// is not added.
+// Esirkepov deposit (src/particle.cpp:427-500) and rho (:503-514) from the
+// three axes' factors.  The last point of each running sum (the sum of all
+// ds, zero up to rounding) is not added.  `moved`: the particle changed
+// position (one at rest adds no current, only rho).
 template <typename real, int P, class Acc>
-__device__ __forceinline__ void deposit(const Acc &acc, const real (&dxdt)[3], const int (&i1)[3],
-                                        const double (&d0)[3], const int (&i2)[3], const double (&d1)[3],
-                                        real qw) {
+__device__ __forceinline__ void deposit(const Acc &acc, const real (&dxdt)[3], const Axis1D<real, P> (&ax)[3],
+                                        bool moved, real qw) {
     constexpr int H = P / 2;
-    int base[3], len[3];
-    real s0[3][P + 1], ds[3][P + 1], w1[3][P];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        double a0[P], a1[P];
-        shape_weights(d0[d], a0);
-        shape_weights(d1[d], a1);
-        span1d<real, P>(i1[d], a0, i2[d], a1, base[d], len[d], s0[d], ds[d]);
-#pragma unroll
-        for (int q = 0; q < P; ++q) w1[d][q] = (real)a1[q];
-    }
+    const int base[3] = {ax[0].base, ax[1].base, ax[2].base};
+    const int len[3] = {ax[0].len, ax[1].len, ax[2].len};
+    const real(&s0x)[P + 1] = ax[0].s0;
+    const real(&s0y)[P + 1] = ax[1].s0;
+    const real(&s0z)[P + 1] = ax[2].s0;
+    const real(&dsx)[P + 1] = ax[0].ds;
+    const real(&dsy)[P + 1] = ax[1].ds;
+    const real(&dsz)[P + 1] = ax[2].ds;
     const real third = real(1.0 / 3.0), half = real(0.5);
     const real cx = qw * dxdt[0] * acc.coef(0), cy = qw * dxdt[1] * acc.coef(1), cz = qw * dxdt[2] * acc.coef(2);
     const int rx = acc.sy, rxy = acc.sz;
@@ -226,24 +305,20 @@ __device__ __forceinline__ void deposit(const Acc &acc, const real (&dxdt)[3], c
     // code overflows the instruction cache (measured 10 % faster rolled),
     // while FP64 and 2nd order run faster unrolled.
     constexpr bool kRollMid = sizeof(real) == 4 && P == 5;
-    // a particle that did not move (every ds zero) adds no current
-    bool moved = false;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) moved = moved || i1[d] != i2[d] || d0[d] != d1[d];
     if (moved) {
         // Jx: running sum of ds along x times the yz weight
 #pragma unroll 1
         for (int k = 0; k < len[2]; ++k) {
-            const real s0z = pick(s0[2], k), dsz = pick(ds[2], k);
-            mid_loop<kRollMid, P>(len[1], s0[1], ds[1], [&](int j, real s0y, real dsy) {
-                const real wyz = s0y * s0z + half * dsy * s0z + half * s0y * dsz + third * dsy * dsz;
+            const real sz0 = pick(s0z, k), szd = pick(dsz, k);
+            mid_loop<kRollMid, P>(len[1], s0y, dsy, [&](int j, real sy0, real syd) {
+                const real wyz = sy0 * sz0 + half * syd * sz0 + half * sy0 * szd + third * syd * szd;
                 const real cw = -cx * wyz;
                 real a = 0;
                 const int row = r0 + k * rxy + j * rx;
 #pragma unroll
                 for (int i = 0; i < P; ++i) {
                     if (i >= len[0] - 1) break;
-                    a += ds[0][i];
+                    a += dsx[i];
                     acc.add(0, row + i, cw * a);
                 }
             });
@@ -251,16 +326,16 @@ __device__ __forceinline__ void deposit(const Acc &acc, const real (&dxdt)[3], c
         // Jy
 #pragma unroll 1
         for (int k = 0; k < len[2]; ++k) {
-            const real s0z = pick(s0[2], k), dsz = pick(ds[2], k);
-            mid_loop<kRollMid, P>(len[0], s0[0], ds[0], [&](int i, real s0x, real dsx) {
-                const real wxz = s0x * s0z + half * dsx * s0z + half * s0x * dsz + third * dsx * dsz;
+            const real sz0 = pick(s0z, k), szd = pick(dsz, k);
+            mid_loop<kRollMid, P>(len[0], s0x, dsx, [&](int i, real sx0, real sxd) {
+                const real wxz = sx0 * sz0 + half * sxd * sz0 + half * sx0 * szd + third * sxd * szd;
                 const real cw = -cy * wxz;
                 real a = 0;
                 const int col = r0 + k * rxy + i;
 #pragma unroll
                 for (int j = 0; j < P; ++j) {
                     if (j >= len[1] - 1) break;
-                    a += ds[1][j];
+                    a += dsy[j];
                     acc.add(1, col + j * rx, cw * a);
                 }
             });
@@ -268,16 +343,16 @@ __device__ __forceinline__ void deposit(const Acc &acc, const real (&dxdt)[3], c
         // Jz
 #pragma unroll 1
         for (int j = 0; j < len[1]; ++j) {
-            const real s0y = pick(s0[1], j), dsy = pick(ds[1], j);
-            mid_loop<kRollMid, P>(len[0], s0[0], ds[0], [&](int i, real s0x, real dsx) {
-                const real wxy = s0x * s0y + half * dsx * s0y + half * s0x * dsy + third * dsx * dsy;
+            const real sy0 = pick(s0y, j), syd = pick(dsy, j);
+            mid_loop<kRollMid, P>(len[0], s0x, dsx, [&](int i, real sx0, real sxd) {
+                const real wxy = sx0 * sy0 + half * sxd * sy0 + half * sx0 * syd + third * sxd * syd;
                 const real cw = -cz * wxy;
                 real a = 0;
                 const int col = r0 + j * rx + i;
 #pragma unroll
                 for (int k = 0; k < P; ++k) {
                     if (k >= len[2] - 1) break;
-                    a += ds[2][k];
+                    a += dsz[k];
                     acc.add(2, col + k * rxy, cw * a);
                 }
             });
@@ -285,15 +360,15 @@ __device__ __forceinline__ void deposit(const Acc &acc, const real (&dxdt)[3], c
     }
     if (acc.has_rho()) {
         const real qwr = qw * acc.coef(3);
-        const int rb = (i2[2] - H) * rxy + (i2[1] - H) * rx + (i2[0] - H) + acc.o;
+        const int rb = (ax[2].i2 - H) * rxy + (ax[1].i2 - H) * rx + (ax[0].i2 - H) + acc.o;
 #pragma unroll 1
         for (int k = 0; k < P; ++k) {
-            const real wk = qwr * pick(w1[2], k);
+            const real wk = qwr * pick(ax[2].w1, k);
 #pragma unroll
             for (int j = 0; j < P; ++j) {
-                real wjk = wk * w1[1][j];
+                real wjk = wk * ax[1].w1[j];
 #pragma unroll
-                for (int i = 0; i < P; ++i) acc.add(3, rb + k * rxy + j * rx + i, wjk * w1[0][i]);
+                for (int i = 0; i < P; ++i) acc.add(3, rb + k * rxy + j * rx + i, wjk * ax[0].w1[i]);
             }
         }
     }
@@ -398,10 +473,11 @@ __device__ __forceinline__ void push_body(const PushArgs<real> &a, long long p, 
     real gam = sqrt(real(1) + (pxn * pxn + pyn * pyn + pzn * pzn));
     // move in cell units (particle.cpp:313-315)
     int i2[3];
-    double d0[3], d2[3];   // primal offsets of the old and new position for the deposit (FP64)
+    double d2[3];   // FP64: new primal offsets
     double xn[3];
     int cn[3];
     real on[3];
+    real disp[3];   // FP32: the move in cells
     if constexpr (F64) {
         xn[0] = o.xd[0] + (double)pxn / (double)gam * a.dt_s / a.dxs[0];
         xn[1] = o.xd[1] + (double)pyn / (double)gam * a.dt_s / a.dxs[1];
@@ -411,10 +487,11 @@ __device__ __forceinline__ void push_body(const PushArgs<real> &a, long long p, 
             double xc = xn[d] - (double)(1 - g.mem);
             i2[d] = (int)(xc + 0.5);
             d2[d] = xc - (double)i2[d];
-            d0[d] = o.dp[d];
         }
     } else {
-        const real disp[3] = {pxn / gam * a.dt_d[0], pyn / gam * a.dt_d[1], pzn / gam * a.dt_d[2]};
+        disp[0] = pxn / gam * a.dt_d[0];
+        disp[1] = pyn / gam * a.dt_d[1];
+        disp[2] = pzn / gam * a.dt_d[2];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             // stored position: cell + FP32 offset in [0, 1)
@@ -428,12 +505,8 @@ __device__ __forceinline__ void push_body(const PushArgs<real> &a, long long p, 
             }
             cn[d] = o.cc[d] + s;
             on[d] = q;
-            // deposit: the unrounded move old offset + displacement, in FP64
-            double u = (double)o.oo[d] + (double)disp[d];
-            double f = floor(u + 0.5);
-            i2[d] = o.cc[d] + g.mem - 1 + (int)f;
-            d2[d] = u - f;
-            d0[d] = (double)o.dp[d];
+            // new primal index of the stored position
+            i2[d] = cn[d] + g.mem - 1 + (q >= real(0.5) ? 1 : 0);
         }
     }
     bool fin = isfinite(pxn) && isfinite(pyn) && isfinite(pzn);
@@ -443,7 +516,22 @@ __device__ __forceinline__ void push_body(const PushArgs<real> &a, long long p, 
         return;
     }
     const real qw = a.charge * a.w[p];
-    deposit<real, P>(acc, a.d_dt, o.ip, d0, i2, d2, qw);
+    Axis1D<real, P> ax[3];
+    bool moved = false;
+    if constexpr (F64) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            axis_from_offsets<real, P>(o.ip[d], o.dp[d], i2[d], d2[d], ax[d]);
+            moved = moved || i2[d] != o.ip[d] || d2[d] != o.dp[d];
+        }
+    } else {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            axis_from_move<P>(o.ip[d], o.dp[d], disp[d], i2[d], ax[d]);
+            moved = moved || disp[d] != real(0);
+        }
+    }
+    deposit<real, P>(acc, a.d_dt, ax, moved, qw);
     // store
     a.px[p] = pxn;
     a.py[p] = pyn;
@@ -533,7 +621,7 @@ inline PushArgs<real> make_push_args(pic_ctx *c, int kind) {
     real **R = (real **)c->ring;
     a.ex = F[0]; a.ey = F[1]; a.ez = F[2]; a.bx = F[3]; a.by = F[4]; a.bz = F[5];
     a.jx = R[0]; a.jy = R[1]; a.jz = R[2];
-    a.rho = c->p.deposit_rho ? R[3 + kind] : nullptr;
+    a.rho = (c->p.deposit_rho && !c->rho_skip) ? R[3 + kind] : nullptr;
     a.count = s.d_count;
     const int cu = s.cur, nx = 1 - s.cur;
     a.x0 = s.a.x[cu]; a.y0 = s.a.y[cu]; a.z0 = s.a.z[cu];

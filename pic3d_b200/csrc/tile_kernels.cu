@@ -63,7 +63,11 @@ __device__ __forceinline__ int cell_key(const TileGeom &t, int cx, int cy, int c
     const int T = t.T;
     int tx = cx / T, ty = cy / T, tz = cz / T;
     int lx = cx - tx * T, ly = cy - ty * T, lz = cz - tz * T;
+#ifdef PIC_SORT_CELL_MAJOR
+    return ((((tz * t.nt[1] + ty) * t.nt[0] + tx) * T + lz) * T * T + ly * T + lx) * kOctants + oct;
+#else
     return ((((tz * t.nt[1] + ty) * t.nt[0] + tx) * kOctants + oct) * T + lz) * T * T + ly * T + lx;
+#endif
 }
 
 // cell of a particle for sorting (FP64: periodic wrap as the next push
@@ -466,7 +470,7 @@ __global__ void __launch_bounds__(tile_threads<real>(), tile_min_blocks<real>())
         int lz = l / D2, r = l - lz * D2, ly = r / DE, lx = r - ly * DE;
         const unsigned *q = sa + c * NL * DS + lz * dsz + ly * dsy + lx;
         long long tot;
-        if constexpr (NL == 2) tot = c >= 3 ? (long long)(int)q[0] : ((long long)(int)q[DS] << 20) + (long long)q[0];
+        if constexpr (NL == 2) tot = ((long long)(int)q[DS] << 20) + (long long)q[0];
         else tot = ((long long)(int)q[2 * DS] << 40) + ((long long)q[DS] << 20) + (long long)q[0];
         if (tot == 0) continue;
         int x = dO[0] + lx, y = dO[1] + ly, z = dO[2] + lz;
@@ -487,7 +491,7 @@ static TileGeom tile_layout(const pic_ctx *c) {
     padded_strides(t.DE, t.T, t.dsy, t.dsz);
     t.gsize = t.GE * t.gsz;
     t.dsize = t.DE * t.dsz;
-    t.nacc = c->p.deposit_rho ? 5 : 3;
+    t.nacc = (c->p.deposit_rho && !c->rho_skip) ? 5 : 3;
     return t;
 }
 
@@ -517,16 +521,9 @@ static void tile_push_t(pic_ctx *c, int mask) {
     const double lim = std::ldexp(1.0, 20 * limbs<real>() - 9);
     const double smax = P == 3 ? 0.75 : 115.0 / 192.0;
     const double bj = 1.01 * qw_max * dmax / c->p.dt, br = 1.01 * qw_max * smax * smax * smax;
-    // FP32 rho is one signed 32-bit word per point: kMaxTileParticles
-    // contributions below 2^19 each cannot overflow.  The resolution, 2^-19
-    // of the largest possible contribution, leaves a point's sum of a few
-    // thousand rounded contributions within about 1e-6 of itself: rho
-    // contributions carry no velocity factor, so (unlike J) they are never
-    // far below their bound
-    const double lim_rho = limbs<real>() == 2 ? std::ldexp(1.0, 19) : lim;
     for (int k = 0; k < 4; ++k) {
         double b = k < 3 ? bj : br;
-        double s = b > 0.0 ? (k < 3 ? lim : lim_rho) / b : 1.0;
+        double s = b > 0.0 ? lim / b : 1.0;
         ta.scale[k] = (real)s;
         ta.inv_scale[k] = 1.0 / (double)ta.scale[k];
     }

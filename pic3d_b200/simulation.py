@@ -128,9 +128,12 @@ class Simulation:
         self._check(self.lib.pic_num_particles(self.ctx, kind, ctypes.byref(n)))
         return n.value
 
-    def download_particles(self, kind: int) -> np.ndarray:
+    def download_particles(self, kind: int, out: np.ndarray | None = None) -> np.ndarray:
+        """The species' records; `out` (PARTICLE_DTYPE, large enough) is
+        reused when given instead of allocating a new array."""
         n = self.num_particles(kind)
-        out = np.empty(n, dtype=PARTICLE_DTYPE)   # every byte is written by the download
+        if out is None or len(out) < n or out.dtype != PARTICLE_DTYPE or not out.flags.c_contiguous:
+            out = np.empty(n, dtype=PARTICLE_DTYPE)   # every byte is written by the download
         got = ctypes.c_int64()
         self._check(self.lib.pic_download_particles(self.ctx, kind, out.ctypes.data if n else None, n,
                                                     ctypes.byref(got)))

@@ -61,6 +61,56 @@ def test_noalloc_diagnostics_match_context_diagnostics():
     sim.close()
 
 
+def test_noalloc_call_allocates_no_device_memory():
+    """After a first call (which loads the module and looks up the scratch
+    address), a call leaves the device's free memory exactly as it was."""
+    import torch
+
+    from pic3d_b200 import _lib as L
+    from pic3d_b200.simulation import Simulation
+
+    lib = L.load()
+    g = load("periodic_o2")
+    sim = Simulation(g["params"], precision="fp64")
+    dev = {n: torch.from_numpy(sim.download_array(n)).to("cuda") for n in FIELDS}
+    sim.close()
+    out = torch.zeros(4, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    assert _noalloc(lib, sim.params, dev, out, stream) == L.PIC_OK
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    assert _noalloc(lib, sim.params, dev, out, stream) == L.PIC_OK
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
+
+
+def test_noalloc_reports_a_nan_field_as_a_nan_gauss_residual():
+    import torch
+
+    from pic3d_b200 import _lib as L
+    from pic3d_b200.simulation import Simulation
+
+    lib = L.load()
+    g = load("periodic_o2")
+    sim = Simulation(g["params"], precision="fp64")
+    for k in range(2):
+        sim.upload_particles(k, g["input"][k])
+    sim.initial_push()
+    sim.run_main_time_loop(1)
+    host = {n: sim.download_array(n) for n in FIELDS}
+    sim.close()
+    m = int(g["params"]["mem"])
+    host["ex"][m + 1, m + 1, m + 1] = float("nan")
+    dev = {n: torch.from_numpy(a).to("cuda") for n, a in host.items()}
+    out = torch.zeros(4, dtype=torch.float64, device="cuda")
+    assert _noalloc(lib, sim.params, dev, out, torch.cuda.current_stream().cuda_stream) == L.PIC_OK
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    assert np.isnan(got[0]) and np.isnan(got[3])
+    assert np.isfinite(got[1]) and np.isfinite(got[2])
+
+
 def test_noalloc_rejects_grids_beyond_the_static_scratch():
     import torch
 
