@@ -542,6 +542,7 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"], help="headline precision")
     ap.add_argument("--cells", default="512,256,256", help="headline grid (smaller grids for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-launch-count", action="store_true", help="skip the CUDA activity trace (for ncu runs)")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-fp32-error", action="store_true")
     ap.add_argument("--no-laser", action="store_true")
@@ -579,7 +580,7 @@ def main():
     ncell = w.nx * w.ny * w.nz
     sim.initial_push()
     sim.run_main_time_loop(args.warmup)
-    launches_per_step = count_kernel_launches(sim, 4)
+    launches_per_step = None if args.no_launch_count else count_kernel_launches(sim, 4)
     clocks = Clocks(local)
     if dist:
         dist.barrier()

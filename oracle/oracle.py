@@ -49,7 +49,7 @@ class OrcState(ctypes.Structure):
         ("waist", _D), ("xfocus", _D), ("yfocus", _D), ("zfocus", _D), ("phase", _D),
         ("E_schwinger", _D),
         ("laser_envelope", _I), ("laser_profile", _I), ("profile_coef", _P(_D)), ("profile_n", _I),
-        ("g_data_size", _I), ("g_data", _P(_D)),
+        ("absorbing", _I), ("g_data_size", _I), ("g_data", _P(_D)),
         ("ex", _P(_D)), ("ey", _P(_D)), ("ez", _P(_D)), ("bx", _P(_D)), ("by", _P(_D)), ("bz", _P(_D)),
         ("jx", _P(_D)), ("jy", _P(_D)), ("jz", _P(_D)), ("rho0", _P(_D)), ("rho1", _P(_D)),
         ("particles", ctypes.c_void_p * 2), ("num_particles", ctypes.c_int64 * 2),
@@ -145,6 +145,7 @@ class Oracle:
                   "E_schwinger"]:
             setattr(s, k, p[k])
         s.laser_envelope = int(p.get("laser_envelope", 0))
+        s.absorbing = int(p.get("absorbing", 0))
         if self.profile is not None:
             s.laser_profile = 1
             s.profile_coef = _dptr(self.profile)

@@ -228,7 +228,7 @@ void orc_radiating_boundary(orc_state *s, int is_left, int is_right, int step) {
                              s->dt / s->dy * (s->bx[FI(g, j, i, m)] - s->bx[FI(g, j, i - 1, m)]) -
                              beta * s->by[FI(g, j, i, m)] + s->dt * s->jz[RI(g, j, i, m)]);
             }
-            if (neighbour(s, 0) == -2) {
+            if (neighbour(s, 0) == -2 && !s->absorbing) {
                 s->bz[FI(g, j, i, L + 1)] =
                     alpha * (-4 * S_r + 2 * s->ey[FI(g, j, i, L)] -
                              s->dt / s->dz * (s->bx[FI(g, j, i, L)] - s->bx[FI(g, j - 1, i, L)]) -
@@ -319,15 +319,67 @@ static void update_b(orc_state *s) {
     orc_exchange_boundary_data(s, s->bz);
 }
 
+/* Extension (absorbing = 1; the reference has none): the first-order
+ * Silver-Mueller condition of radiating_boundary's x-min update
+ * (src/boundary.cpp:88-89) on the other non-periodic faces, after every B
+ * half-update.  Min faces (y, z) set the ghost B row mem-1 with the x-min
+ * formula's axes relabelled cyclically; max faces (y, z, x) set the last
+ * physical B row, reflected through the face (tangential B flips sign; E,
+ * J and the normal B do not), from the E and J of that row and the B row
+ * below it.  alpha = 1/(1 + dt/h), beta = 1 - dt/h, h the cell size across
+ * the face. */
+static void absorb_faces(orc_state *s) {
+    if (!s->absorbing) return;
+    geom g = make_geom(s);
+    const int m = s->mem;
+    const double dt = s->dt, hx = s->dt / s->dx, hy = s->dt / s->dy, hz = s->dt / s->dz;
+    for (int face = 0; face < 5; ++face) {
+        const int ax = face < 2 ? 1 : (face < 4 ? 2 : 0);
+        if (neighbour(s, ax) != -2) continue;
+        const int lo = face == 0 || face == 2;
+        const double h = ax == 0 ? hx : (ax == 1 ? hy : hz);
+        const double alpha = 1.0 / (1.0 + h), beta = 1.0 - h, sg = lo ? 1.0 : -1.0;
+        const int row = lo ? m : g.n[ax] + m - 1;
+        for (int k = g.nc_st[2]; k <= g.nc_end[2]; k++)
+            for (int j = g.nc_st[1]; j <= g.nc_end[1]; j++)
+                for (int i = g.nc_st[0]; i <= g.nc_end[0]; i++) {
+                    int q[3] = {i, j, k};
+                    if (q[ax] != row) continue;
+                    int t[3] = {i, j, k}, n[3] = {i, j, k};
+                    if (lo) t[ax] -= 1; else n[ax] -= 1;   /* target row and the interior B row */
+                    long c = FI(g, k, j, i), rc = RI(g, k, j, i);
+                    long ct = FI(g, t[2], t[1], t[0]), cn = FI(g, n[2], n[1], n[0]);
+                    if (ax == 1) {
+                        s->bx[ct] = alpha * (sg * (-2.0 * s->ez[c] - hx * (s->by[c] - s->by[FI(g, k, j, i - 1)]) -
+                                                   dt * s->jz[rc]) - beta * s->bx[cn]);
+                        s->bz[ct] = alpha * (sg * (2.0 * s->ex[c] + hz * (s->by[c] - s->by[FI(g, k - 1, j, i)]) +
+                                                   dt * s->jx[rc]) - beta * s->bz[cn]);
+                    } else if (ax == 2) {
+                        s->by[ct] = alpha * (sg * (-2.0 * s->ex[c] - hy * (s->bz[c] - s->bz[FI(g, k, j - 1, i)]) -
+                                                   dt * s->jx[rc]) - beta * s->by[cn]);
+                        s->bx[ct] = alpha * (sg * (2.0 * s->ey[c] + hx * (s->bz[c] - s->bz[FI(g, k, j, i - 1)]) +
+                                                   dt * s->jy[rc]) - beta * s->bx[cn]);
+                    } else {
+                        s->bz[ct] = alpha * (sg * (-2.0 * s->ey[c] - hz * (s->bx[c] - s->bx[FI(g, k - 1, j, i)]) -
+                                                   dt * s->jy[rc]) - beta * s->bz[cn]);
+                        s->by[ct] = alpha * (sg * (2.0 * s->ez[c] + hy * (s->bx[c] - s->bx[FI(g, k, j - 1, i)]) +
+                                                   dt * s->jz[rc]) - beta * s->by[cn]);
+                    }
+                }
+    }
+}
+
 /* update_electromagnetic_fields_first: src/field.cpp:56-86 */
 void orc_fields_first(orc_state *s) {
     update_e(s);
     update_b(s);
+    absorb_faces(s);
 }
 
 /* update_electromagnetic_fields_second: src/field.cpp:88-117 */
 void orc_fields_second(orc_state *s) {
     update_b(s);
+    absorb_faces(s);
     update_e(s);
 }
 

@@ -50,6 +50,7 @@ typedef struct orc_state {
     int32_t laser_profile;       /* 0: Gaussian beam (boundary.cpp:38), 1: bicubic amplitude grid */
     const double *profile_coef;  /* profile_n x profile_n coefficients over the physical y-z face */
     int32_t profile_n;
+    int32_t absorbing;           /* 1: Silver-Mueller absorbing condition on the non-periodic y, z and x-max faces */
     int32_t g_data_size;
     const double *g_data;        /* g-factor table (reference g.txt), may be NULL when unused */
     /* arrays */

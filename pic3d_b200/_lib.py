@@ -36,6 +36,7 @@ class PicParams(ctypes.Structure):
         ("capacity", _I64 * 2),
         ("precision", _I32), ("spin", _I32), ("deposit_rho", _I32),
         ("laser_envelope", _I32), ("laser_profile", _I32), ("tile", _I32), ("sort_interval", _I32), ("adjoint", _I32),
+        ("absorbing", _I32),
     ]
 
 

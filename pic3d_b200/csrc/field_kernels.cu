@@ -247,6 +247,7 @@ struct LaserArgs {
     const double *coef;
     double time;
     int is_left, is_right;
+    int absorbing;   // extension: the x-max face takes the absorbing condition instead
 };
 
 __device__ double laser_envelope(const LaserArgs &L, double time, double position) {
@@ -325,7 +326,7 @@ __global__ void radiating_boundary_kernel(Geom g, LaserArgs L, const real *__res
         by[o] = (real)(alpha * (-4 * P_l + 2 * (double)ez[c] + L.dt / L.dy * ((double)bx[c] - (double)bx[c - g.f[0]]) -
                                 beta * (double)by[c] + L.dt * (double)jz[rc]));
     }
-    {
+    if (!L.absorbing) {
         // the reference writes column local_xcells+1 (boundary.cpp:92-96)
         int c = g.fi(iz, iy, xr), o = g.fi(iz, iy, xr + 1), rc = g.ri(iz, iy, xr);
         bz[o] = (real)(alpha * (-4 * S_r + 2 * (double)ey[c] - L.dt / L.dz * ((double)bx[c] - (double)bx[c - g.fxy]) -
@@ -333,6 +334,98 @@ __global__ void radiating_boundary_kernel(Geom g, LaserArgs L, const real *__res
         by[o] = (real)(alpha * (4 * P_r - 2 * (double)ez[c] + L.dt / L.dy * ((double)bx[c] - (double)bx[c - g.f[0]]) -
                                 beta * (double)by[c] - L.dt * (double)jz[rc]));
     }
+}
+
+// ---------------------------------------------------------------------------
+// Absorbing faces (extension, PicParams.absorbing = 1).  The reference
+// absorbs only at x-min, with the Silver-Mueller update of the ghost B
+// column above; its y and z ghosts stay zero (a conductor).  The same
+// first-order condition is applied on every other non-periodic face:
+//   * y-min / z-min: the ghost B row mem-1 from the first physical row, the
+//     reference's x-min update with the axes relabelled cyclically
+//     (x -> y -> z -> x, then once more);
+//   * y-max / z-max / x-max: the last physical B row, whose own update read
+//     the zero ghost E row above it, from the physical E and J of that row
+//     and the B row below: the min-face update reflected through the face
+//     (tangential B changes sign under the reflection, E, J and the normal
+//     B do not).
+// alpha = 1/(1 + dt/h), beta = 1 - dt/h with h the cell size across the
+// face.  Applied after each B half-update, before B is next read.  One
+// thread per point of a face's physical rows; faces are separate launches
+// (edge rows are written by one face each).
+
+struct AbsorbArgs {
+    double dt, idt[3];   // dt and dt/dx, dt/dy, dt/dz
+    int face;            // 0 y-min, 1 y-max, 2 z-min, 3 z-max, 4 x-max
+};
+
+template <typename real>
+__global__ void absorb_face_kernel(Geom g, AbsorbArgs A, const real *__restrict__ ex, const real *__restrict__ ey,
+                                   const real *__restrict__ ez, real *bx, real *by, real *bz,
+                                   const real *__restrict__ jx, const real *__restrict__ jy,
+                                   const real *__restrict__ jz) {
+    // the two in-face axes of this face
+    const int ax = A.face < 2 ? 1 : (A.face < 4 ? 2 : 0);
+    const int u_ax = ax == 0 ? 1 : 0, v_ax = ax == 2 ? 1 : 2;
+    int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y * blockDim.y + threadIdx.y;
+    if (u >= g.n[u_ax] || v >= g.n[v_ax]) return;
+    int q[3];
+    q[u_ax] = u + g.mem;
+    q[v_ax] = v + g.mem;
+    const bool lo = A.face == 0 || A.face == 2;
+    q[ax] = lo ? g.mem : g.n[ax] + g.mem - 1;   // physical row next to the face
+    const int st[3] = {1, g.f[0], g.fxy};
+    const int c = g.fi(q[2], q[1], q[0]), rc = g.ri(q[2], q[1], q[0]);
+    const double h = A.idt[ax];
+    const double alpha = 1.0 / (1.0 + h), beta = 1.0 - h, dt = A.dt;
+    const double sgn = lo ? 1.0 : -1.0;
+    // target B index: ghost row below (min face) or this row (max face);
+    // the interior B used by the update: this row (min) or the row below (max)
+    const int tgt = lo ? c - st[ax] : c, inn = lo ? c : c - st[ax];
+    if (ax == 1) {        // y faces: bx from ez, jz, d(by)/dx; bz from ex, jx, d(by)/dz
+        bx[tgt] = (real)(alpha * (sgn * (-2.0 * (double)ez[c] - A.idt[0] * ((double)by[c] - (double)by[c - 1]) -
+                                         dt * (double)jz[rc]) - beta * (double)bx[inn]));
+        bz[tgt] = (real)(alpha * (sgn * (2.0 * (double)ex[c] + A.idt[2] * ((double)by[c] - (double)by[c - g.fxy]) +
+                                         dt * (double)jx[rc]) - beta * (double)bz[inn]));
+    } else if (ax == 2) { // z faces: by from ex, jx, d(bz)/dy; bx from ey, jy, d(bz)/dx
+        by[tgt] = (real)(alpha * (sgn * (-2.0 * (double)ex[c] - A.idt[1] * ((double)bz[c] - (double)bz[c - g.f[0]]) -
+                                         dt * (double)jx[rc]) - beta * (double)by[inn]));
+        bx[tgt] = (real)(alpha * (sgn * (2.0 * (double)ey[c] + A.idt[0] * ((double)bz[c] - (double)bz[c - 1]) +
+                                         dt * (double)jy[rc]) - beta * (double)bx[inn]));
+    } else {              // x-max: the reference's x-min update (boundary.cpp:88-89) reflected
+        bz[tgt] = (real)(alpha * (sgn * (-2.0 * (double)ey[c] - A.idt[2] * ((double)bx[c] - (double)bx[c - g.fxy]) -
+                                         dt * (double)jy[rc]) - beta * (double)bz[inn]));
+        by[tgt] = (real)(alpha * (sgn * (2.0 * (double)ez[c] + A.idt[1] * ((double)bx[c] - (double)bx[c - g.f[0]]) +
+                                         dt * (double)jz[rc]) - beta * (double)by[inn]));
+    }
+}
+
+template <typename real>
+static void absorb_faces(pic_ctx *c) {
+    const Geom &g = c->g;
+    real **F = (real **)c->field;
+    real **R = (real **)c->ring;
+    AbsorbArgs A{};
+    A.dt = c->p.dt;
+    A.idt[0] = c->p.dt / c->p.dx;
+    A.idt[1] = c->p.dt / c->p.dy;
+    A.idt[2] = c->p.dt / c->p.dz;
+    for (int face = 0; face < 5; ++face) {
+        const int ax = face < 2 ? 1 : (face < 4 ? 2 : 0);
+        if (g.per[ax]) continue;
+        const int u_ax = ax == 0 ? 1 : 0, v_ax = ax == 2 ? 1 : 2;
+        A.face = face;
+        dim3 blk(32, 8), grd((g.n[u_ax] + 31) / 32, (g.n[v_ax] + 7) / 8);
+        absorb_face_kernel<real><<<grd, blk, 0, c->stream>>>(g, A, F[0], F[1], F[2], F[3], F[4], F[5], R[0], R[1],
+                                                             R[2]);
+    }
+}
+
+void launch_absorbing_faces(pic_ctx *c) {
+    if (c->p.absorbing != 1) return;
+    prof_begin(c, "absorbing_faces");
+    if (c->fp32) absorb_faces<float>(c); else absorb_faces<double>(c);
+    prof_end(c);
 }
 
 // ---------------------------------------------------------------------------
@@ -389,6 +482,7 @@ void launch_update_b(pic_ctx *c, double coef) {
     prof_begin(c, "ghost_fill");
     ghost_fill_any(c, c->field[3], c->field[4], c->field[5]);
     prof_end(c);
+    launch_absorbing_faces(c);
 }
 
 void launch_ghost_fill_one(pic_ctx *c, int array) {
@@ -469,6 +563,7 @@ static LaserArgs laser_args(const pic_ctx *c, double time) {
     L.profile = (p.laser_profile == 1 && c->d_profile) ? 1 : 0;
     L.profile_n = c->profile_n; L.coef = c->d_profile;
     L.time = time;
+    L.absorbing = p.absorbing == 1 ? 1 : 0;
     return L;
 }
 

@@ -368,6 +368,7 @@ int pic_create(const PicParams *pp, int device, pic_ctx **out) {
         if (!(p.dt > 0.0) || !(p.dt < d[k])) return bad("dt must satisfy 0 < dt < min(dx,dy,dz) (a particle moves less than a cell per step)");
     }
     if (!(p.mass[0] > 0.0) || !(p.mass[1] > 0.0)) return bad("species masses must be positive");
+    if (p.absorbing != 0 && p.absorbing != 1) return bad("absorbing must be 0 or 1");
     for (int k = 0; k < 3; ++k)
         if (n[k] < 1 || n[k] > (1 << 20)) return bad("cell counts must lie in [1, 2^20]");
     c->g = make_geom(p);
@@ -387,6 +388,7 @@ int pic_create(const PicParams *pp, int device, pic_ctx **out) {
         // no sorting, removal only marks particles dead
         if (p.rank_period[0] || p.rank_period[1] || p.rank_period[2])
             return bad("the adjoint supports absorbing faces only");
+        if (p.absorbing) return bad("the adjoint has no transpose of the absorbing-faces extension");
         c->tile = 0;
     }
     c->sort_interval = p.sort_interval > 0 ? p.sort_interval : 4;
@@ -991,7 +993,7 @@ int pic_save(pic_ctx *c, const char *path) {
     if (!c || !path) return PIC_EINVAL;
     FILE *f = std::fopen(path, "wb");
     if (!f) return fail(c, PIC_EINVAL, std::string("cannot open ") + path);
-    const char magic[8] = {'P', 'I', 'C', '3', 'D', 'B', '2', '1'};
+    const char magic[8] = {'P', 'I', 'C', '3', 'D', 'B', '2', '2'};
     std::fwrite(magic, 1, 8, f);
     std::fwrite(&c->p, sizeof(PicParams), 1, f);
     std::fwrite(&c->step, sizeof(int), 1, f);
@@ -1022,7 +1024,7 @@ int pic_load(pic_ctx *c, const char *path) {
     char magic[8];
     PicParams p;
     int step = 0;
-    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "PIC3DB21", 8) == 0 &&
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "PIC3DB22", 8) == 0 &&
               std::fread(&p, sizeof p, 1, f) == 1 && std::fread(&step, sizeof(int), 1, f) == 1;
     if (!ok || p.local_xcells != c->p.local_xcells || p.local_ycells != c->p.local_ycells ||
         p.local_zcells != c->p.local_zcells || p.mem != c->p.mem) {

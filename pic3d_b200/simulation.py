@@ -45,6 +45,7 @@ def params_from(w, precision: str | None = None, spin: bool = True, deposit_rho:
     pp.tile = int(tile)
     pp.sort_interval = int(sort_interval)
     pp.adjoint = 1 if adjoint else 0
+    pp.absorbing = int(p.get("absorbing", 0))
     pp.charge[0], pp.mass[0] = -1.0, 1.0
     pp.charge[1], pp.mass[1] = 1.0, 1836.0
     return pp

@@ -64,6 +64,7 @@ class Workload:
     zfocus: Optional[float] = None
     phase: float = 0.0
     laser_envelope: int = 0             # 0 reference sine envelope, 1 Gaussian (extension)
+    absorbing: int = 0                  # 1: absorbing y, z and x-max faces (extension)
     steps: int = 200
     precision: str = "fp64"
     E_schwinger: float = 4.1215e5
@@ -103,7 +104,7 @@ class Workload:
             yfocus=self.yfocus if self.yfocus is not None else 0.5 * Ly,
             zfocus=self.zfocus if self.zfocus is not None else 0.5 * Lz,
             phase=self.phase, E_schwinger=self.E_schwinger,
-            laser_envelope=int(self.laser_envelope),
+            laser_envelope=int(self.laser_envelope), absorbing=int(self.absorbing),
         )
 
     def species(self, kind: int) -> dict:
@@ -186,13 +187,15 @@ def laser_underdense(nx=256, ny=128, nz=128, precision="fp64", steps=3000) -> Wo
     """Laser in underdense plasma: dx = lambda/20, dy = dz = lambda/10,
     electrons + protons at 8 per cell each, density 0.01 n_c after a 20 lambda
     linear ramp, cold; linearly polarised pulse a0 = 2, waist 8 lambda,
-    10 lambda/c duration, injected from x-min; absorbing boundaries; 4th-order
-    shape."""
+    Gaussian temporal envelope with an intensity FWHM of 10 lambda/c
+    (extension; the reference has the sine envelope only), injected from
+    x-min; absorbing faces on every side (x-min is the reference's own;
+    y, z and x-max are the extension); 4th-order shape."""
     return Workload(name=f"laser_underdense_{nx}x{ny}x{nz}_{precision}", nx=nx, ny=ny, nz=nz, mem=4,
                     period=(0, 0, 0), dx=LAMBDA / 20, dy=LAMBDA / 10, dz=LAMBDA / 10, ppc=(8, 8),
                     u_th=(0.0, 0.0), density=_ramp(20 * LAMBDA, 0.01), density_value=0.01,
                     laser_amplitude=2.0, laser_pulse_duration=10.0 * LAMBDA, waist=8.0 * LAMBDA,
-                    laser_polarization=1, steps=steps, precision=precision)
+                    laser_polarization=1, laser_envelope=1, absorbing=1, steps=steps, precision=precision)
 
 
 def thermal_scaleup(nx=512, ny=256, nz=256, mem=2, precision="fp32", steps=100) -> Workload:

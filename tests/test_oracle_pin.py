@@ -5,6 +5,8 @@ The golden vectors were produced by the reference's own sources
 every particle record bit for bit, including the particle order that the
 reference's exchange produces (src/mpi_utils.cpp:62-230).
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -70,3 +72,22 @@ def test_shape_known_values():
     # x on a node: quadratic weights 1/8, 3/4, 1/8; quartic 1/384*(1,76,230,76,1)
     np.testing.assert_allclose(O.shape_function(2, 5.0), [0.125, 0.75, 0.125], rtol=0, atol=1e-15)
     np.testing.assert_allclose(O.shape_function(4, 5.0), np.array([1, 76, 230, 76, 1]) / 384.0, atol=1e-15)
+
+
+@pytest.mark.skipif(not (O.have_reference_build() and os.path.exists(O.REF_BIN_O0)),
+                    reason="reference build not present (built where the reference tree is available)")
+@pytest.mark.parametrize("case", ["periodic_o2", "laser_o4", "mixed_o2", "spin_o2"])
+def test_reference_O0_and_O2_builds_dump_identical_states(case):
+    """The reference's own Makefile builds at -O0; the oracle build uses -O2
+    -ffp-contract=off.  Both produce bit-identical per-step dumps, so the
+    faster build stands for the shipped one."""
+    g = load(case)
+    w = g["params"]
+    s2, _ = O.run_reference(w, g["input"], g["steps"])
+    s0, _ = O.run_reference(w, g["input"], g["steps"], binary=O.REF_BIN_O0)
+    assert len(s0) == len(s2)
+    for a, b in zip(s0, s2):
+        for n in ARRAYS:
+            assert a[n].tobytes() == b[n].tobytes(), n
+        for k in range(2):
+            assert a["particles"][k].tobytes() == b["particles"][k].tobytes()
