@@ -713,6 +713,18 @@ __global__ void adj_seed_kinetic_kernel(Geom g, CellPack cp, int fp32, long long
 
 }  // namespace pic
 
+// moves of per-particle arrays between orders (bit copies)
+template <typename T>
+__global__ void scatter_to_kernel(const T *in, const int *to, T *out, long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[to[i]] = in[i];
+}
+template <typename T>
+__global__ void gather_from_kernel(const T *in, const int *from, T *out, long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = in[from[i]];
+}
+
 // ===========================================================================
 // host side: checkpoints, tape and the C ABI
 // ===========================================================================
@@ -726,6 +738,8 @@ struct Blob {
     int step = 0;
     int cur[2] = {0, 0};
     long long count[2] = {0, 0};
+    int field_part = 0;          // tape: index of the first of the six field parts
+    int perm_part[2] = {-1, -1}; // tape: the sort permutation run right before this push, per species
 };
 
 struct AdjState {
@@ -741,6 +755,12 @@ struct AdjState {
     double *lprof = nullptr;
     double *loss = nullptr;
     int nprof = 0;
+    // tiled contexts: upload index of each particle in the order the
+    // per-particle adjoints are held in (valid once seeded), and scratch
+    int *lam_orig[2] = {};
+    bool lam_valid = false;
+    void *tmp = nullptr;
+    size_t tmp_bytes = 0;
 };
 
 static std::vector<std::pair<pic_ctx *, AdjState *>> g_adj;
@@ -776,6 +796,22 @@ static void particle_parts(pic_ctx *c, std::vector<std::pair<void *, size_t>> &v
         v.push_back({s.a.pz, n * rsize(c)});
         if (s.dead) v.push_back({s.dead, n});
     }
+}
+
+// a checkpoint additionally holds what a sort moves but the tape need not:
+// weights, ids and upload indices (tiled contexts)
+static void checkpoint_parts(pic_ctx *c, std::vector<std::pair<void *, size_t>> &v) {
+    particle_parts(c, v);
+    for (int k = 0; k < 2; ++k) {
+        Species &s = c->sp[k];
+        size_t n = (size_t)s.n_host;
+        if (n == 0 || !s.orig) continue;
+        v.push_back({s.a.w, n * rsize(c)});
+        v.push_back({s.a.id, n * sizeof(int)});
+        v.push_back({s.orig, n * sizeof(int)});
+    }
+    for (int f = 0; f < 6; ++f) v.push_back({c->field[f], (size_t)c->g.fsz * rsize(c)});
+    for (int f = 0; f < 5; ++f) v.push_back({c->ring[f], (size_t)c->g.rsz * rsize(c)});
 }
 
 static int blob_save(pic_ctx *c, Blob &b, const std::vector<std::pair<void *, size_t>> &parts) {
@@ -823,9 +859,24 @@ void adjoint_record_hook(pic_ctx *c) {
     }
     std::vector<std::pair<void *, size_t>> parts;
     particle_parts(c, parts);
+    const int field_part = (int)parts.size();
     for (int f = 0; f < 6; ++f) parts.push_back({c->field[f], (size_t)c->g.fsz * rsize(c)});
+    int perm_part[2] = {-1, -1};
+    for (int k = 0; k < 2; ++k) {
+        Species &s = c->sp[k];
+        if (!s.perm_fresh || s.n_host == 0) continue;
+        perm_part[k] = (int)parts.size();
+        parts.push_back({s.perm, (size_t)s.n_host * sizeof(int)});
+        s.perm_fresh = false;
+    }
     prof_begin(c, "adjoint_tape_record");
-    if (blob_save(c, A->tape[A->tape_len], parts) == PIC_OK) A->tape_len++;
+    Blob &b = A->tape[A->tape_len];
+    if (blob_save(c, b, parts) == PIC_OK) {
+        b.field_part = field_part;
+        b.perm_part[0] = perm_part[0];
+        b.perm_part[1] = perm_part[1];
+        A->tape_len++;
+    }
     prof_end(c);
 }
 }  // namespace pic
@@ -846,6 +897,17 @@ static int ensure_adj_arrays(pic_ctx *c, AdjState *A) {
         ok = ok && alloc((void **)&A->lw[k], n * sizeof(double));
     }
     ok = ok && alloc((void **)&A->loss, sizeof(double));
+    if (c->sp[0].orig || c->sp[1].orig) {
+        size_t n = (size_t)std::max<int64_t>(std::max(c->sp[0].cap, c->sp[1].cap), 1);
+        for (int k = 0; k < 2; ++k) ok = ok && alloc((void **)&A->lam_orig[k], n * sizeof(int));
+        if (A->tmp_bytes < n * sizeof(double)) {
+            if (A->tmp) cudaFree(A->tmp);
+            A->tmp = nullptr;
+            A->tmp_bytes = 0;
+        }
+        ok = ok && alloc(&A->tmp, n * sizeof(double));
+        if (ok) A->tmp_bytes = n * sizeof(double);
+    }
     int np = std::max(c->profile_n * c->profile_n, 1);
     if (A->nprof != np && A->lprof) {
         cudaFree(A->lprof);
@@ -858,6 +920,73 @@ static int ensure_adj_arrays(pic_ctx *c, AdjState *A) {
         return PIC_ENOMEM;
     }
     return PIC_OK;
+}
+
+// the per-particle arrays a sort moves that the reverse sweep reads:
+// position and momentum adjoints, weight adjoint, weights, upload index
+static int moved_arrays(pic_ctx *c, AdjState *A, int k, void **arr, size_t *es) {
+    int m = 0;
+    for (int q = 0; q < 6; ++q) { arr[m] = A->lpart[k][q]; es[m++] = rsize(c); }
+    arr[m] = A->lw[k]; es[m++] = sizeof(double);
+    arr[m] = c->sp[k].a.w; es[m++] = rsize(c);
+    arr[m] = c->sp[k].orig; es[m++] = sizeof(int);
+    return m;
+}
+
+static void scatter_to(pic_ctx *c, const void *in, const int *to, void *out, size_t es, long long n) {
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+    if (es == 8) scatter_to_kernel<unsigned long long><<<blocks, 256, 0, c->stream>>>(
+        (const unsigned long long *)in, to, (unsigned long long *)out, n);
+    else scatter_to_kernel<unsigned><<<blocks, 256, 0, c->stream>>>((const unsigned *)in, to, (unsigned *)out, n);
+}
+
+static void gather_from(pic_ctx *c, const void *in, const int *from, void *out, size_t es, long long n) {
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+    if (es == 8) gather_from_kernel<unsigned long long><<<blocks, 256, 0, c->stream>>>(
+        (const unsigned long long *)in, from, (unsigned long long *)out, n);
+    else gather_from_kernel<unsigned><<<blocks, 256, 0, c->stream>>>((const unsigned *)in, from, (unsigned *)out, n);
+}
+
+// undo one recorded sort of species k (perm[new] = old): every moved array
+// goes back to the order before that sort
+static void unsort_species(pic_ctx *c, AdjState *A, int k, const int *perm, long long n) {
+    void *arr[9];
+    size_t es[9];
+    const int m = moved_arrays(c, A, k, arr, es);
+    for (int q = 0; q < m; ++q) {
+        cudaMemcpyAsync(A->tmp, arr[q], (size_t)n * es[q], cudaMemcpyDeviceToDevice, c->stream);
+        scatter_to(c, A->tmp, perm, arr[q], es[q], n);
+    }
+}
+
+// the adjoints are held in the order given by lam_orig (upload indices);
+// bring them into the context's current order (its orig array): a segment
+// recomputed from a checkpoint sorts again and need not end in the order
+// the later segment's reverse sweep started from
+static void remap_adjoints(pic_ctx *c, AdjState *A) {
+    if (!A->lam_valid) return;
+    for (int k = 0; k < 2; ++k) {
+        Species &s = c->sp[k];
+        const long long n = s.n_host;
+        if (!s.orig || n == 0) continue;
+        void *arr[9];
+        size_t es[9];
+        const int m = moved_arrays(c, A, k, arr, es) - 2;   // the adjoints only (weights, orig are current)
+        for (int q = 0; q < m; ++q) {
+            scatter_to(c, arr[q], A->lam_orig[k], A->tmp, es[q], n);
+            gather_from(c, A->tmp, s.orig, arr[q], es[q], n);
+        }
+    }
+}
+
+static void note_adjoint_order(pic_ctx *c, AdjState *A) {
+    for (int k = 0; k < 2; ++k) {
+        Species &s = c->sp[k];
+        if (s.orig && s.n_host > 0)
+            cudaMemcpyAsync(A->lam_orig[k], s.orig, (size_t)s.n_host * sizeof(int), cudaMemcpyDeviceToDevice,
+                            c->stream);
+    }
+    A->lam_valid = c->sp[0].orig || c->sp[1].orig;
 }
 
 template <typename real, int P>
@@ -882,8 +1011,7 @@ static void adj_push_launch(pic_ctx *c, AdjState *A, const Blob &b, int kind, in
     a.py = (const real *)blob_part(b, idx++);
     a.pz = (const real *)blob_part(b, idx++);
     a.dead = s.dead ? (const unsigned char *)blob_part(b, idx++) : nullptr;
-    const int nparts = (int)b.parts.size();
-    for (int f = 0; f < 6; ++f) a.f[f] = (const real *)blob_part(b, nparts - 6 + f);
+    for (int f = 0; f < 6; ++f) a.f[f] = (const real *)blob_part(b, b.field_part + f);
     a.w = (const real *)s.a.w;
     for (int f = 0; f < 3; ++f) a.lj[f] = (const real *)A->lj[f];
     for (int f = 0; f < 6; ++f) a.lf[f] = (real *)A->lf[f];
@@ -976,6 +1104,9 @@ static int adj_backward_t(pic_ctx *c, AdjState *A, int nsteps) {
             if (c->order == 2) adj_push_launch<real, 3>(c, A, b, k, base[k], loop);
             else adj_push_launch<real, 5>(c, A, b, k, base[k], loop);
         }
+        // the push ran right after a sort: back to the order before it
+        for (int k = 0; k < 2; ++k)
+            if (b.perm_part[k] >= 0) unsort_species(c, A, k, (const int *)blob_part(b, b.perm_part[k]), b.count[k]);
         // clear_currents: J before the clear does not reach the deposit
         prof_begin(c, "adjoint_clear");
         for (int f = 0; f < 3; ++f) cudaMemsetAsync(A->lj[f], 0, (size_t)c->g.rsz * rsize(c), c->stream);
@@ -1002,9 +1133,7 @@ int pic_checkpoint_save(pic_ctx *c, int slot) {
     AdjState *A = adj_of(c, true);
     if ((int)A->ckpt.size() <= slot) A->ckpt.resize(slot + 1);
     std::vector<std::pair<void *, size_t>> parts;
-    particle_parts(c, parts);
-    for (int f = 0; f < 6; ++f) parts.push_back({c->field[f], (size_t)c->g.fsz * rsize(c)});
-    for (int f = 0; f < 5; ++f) parts.push_back({c->ring[f], (size_t)c->g.rsz * rsize(c)});
+    checkpoint_parts(c, parts);
     return blob_save(c, A->ckpt[slot], parts);
 }
 
@@ -1023,10 +1152,21 @@ int pic_checkpoint_restore(pic_ctx *c, int slot) {
         }
         c->sp[k].cur = b.cur[k];
     }
+    // the arrays' current buffers (a sort since the save may have swapped them)
+    std::vector<std::pair<void *, size_t>> parts;
+    checkpoint_parts(c, parts);
+    if (parts.size() != b.parts.size()) {
+        c->err = "checkpoint layout differs from the context's";
+        return PIC_EINVAL;
+    }
     size_t off = 0;
-    for (auto &p : b.parts) {
-        cudaMemcpyAsync(p.first, (char *)b.buf + off, p.second, cudaMemcpyDeviceToDevice, c->stream);
-        off += (p.second + 255) & ~(size_t)255;
+    for (size_t i = 0; i < parts.size(); ++i) {
+        cudaMemcpyAsync(parts[i].first, (char *)b.buf + off, parts[i].second, cudaMemcpyDeviceToDevice, c->stream);
+        off += (parts[i].second + 255) & ~(size_t)255;
+    }
+    for (int k = 0; k < 2; ++k) {
+        c->sp[k].sorted = false;   // the next push sorts (and the tape records that permutation)
+        c->sp[k].perm_fresh = false;
     }
     c->step = b.step;
     return PIC_OK;
@@ -1088,6 +1228,7 @@ int pic_adjoint_seed_kinetic(pic_ctx *c, int kind, double xlo, double xhi, doubl
                 (double *)s.a.pz, (double *)s.a.w, s.dead, c->p.mass[kind], xlo, xhi, ramp, (double *)A->lpart[kind][0], (double *)A->lpart[kind][3],
                 (double *)A->lpart[kind][4], (double *)A->lpart[kind][5], A->lw[kind], A->loss);
     }
+    note_adjoint_order(c, A);
     double l = 0.0;
     cudaMemcpyAsync(&l, A->loss, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return PIC_ECUDA;
@@ -1102,7 +1243,10 @@ int pic_adjoint_backward(pic_ctx *c, int nsteps) {
         c->err = "adjoint: seed the objective first";
         return PIC_EINVAL;
     }
-    return c->fp32 ? adj_backward_t<float>(c, A, nsteps) : adj_backward_t<double>(c, A, nsteps);
+    remap_adjoints(c, A);
+    int r = c->fp32 ? adj_backward_t<float>(c, A, nsteps) : adj_backward_t<double>(c, A, nsteps);
+    note_adjoint_order(c, A);
+    return r;
 }
 
 int pic_adjoint_weight_grad(pic_ctx *c, int kind, double *out, int64_t n) {
@@ -1110,7 +1254,13 @@ int pic_adjoint_weight_grad(pic_ctx *c, int kind, double *out, int64_t n) {
     AdjState *A = adj_of(c, false);
     if (!A || !A->lw[kind]) return PIC_EINVAL;
     if (n > c->sp[kind].n_host) n = c->sp[kind].n_host;
-    cudaMemcpyAsync(out, A->lw[kind], (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    const double *src = A->lw[kind];
+    Species &s = c->sp[kind];
+    if (s.orig && n > 0 && s.n_host > 0) {   // sorted context: back to upload order
+        scatter_to(c, A->lw[kind], s.orig, A->tmp, sizeof(double), s.n_host);
+        src = (const double *)A->tmp;
+    }
+    cudaMemcpyAsync(out, src, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
     return cudaStreamSynchronize(c->stream) == cudaSuccess ? PIC_OK : PIC_ECUDA;
 }
 
@@ -1138,6 +1288,8 @@ int pic_adjoint_release(pic_ctx *c) {
         for (double *p : A->lw) if (p) cudaFree(p);
         if (A->lprof) cudaFree(A->lprof);
         if (A->loss) cudaFree(A->loss);
+        for (int *p : A->lam_orig) if (p) cudaFree(p);
+        if (A->tmp) cudaFree(A->tmp);
         delete A;
         g_adj.erase(g_adj.begin() + (long)i);
         return PIC_OK;

@@ -606,6 +606,15 @@ __global__ void deposit_one_kernel(PushArgs<real> a, double xo, double yo, doubl
     deposit<real, P>(acc, a.d_dt, ax, moved, (real)qw);
 }
 
+__global__ void iota_kernel(int *a, long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = (int)i;
+}
+
+void launch_iota(pic_ctx *c, int *a, long long n) {
+    iota_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(a, n);
+}
+
 void launch_deposit_one(pic_ctx *c, int kind, const double (&xo)[3], const double (&xn)[3], double qw) {
     if (c->fp32) {
         PushArgs<float> a = make_push_args<float>(c, kind);

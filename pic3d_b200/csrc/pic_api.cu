@@ -69,6 +69,9 @@ void free_species(Species &s) {
     if (s.keys) cudaFree(s.keys);
     if (s.strag) cudaFree(s.strag);
     if (s.dead) cudaFree(s.dead);
+    void *adj[4] = {s.orig, s.orig_b, s.dead_b, s.perm};
+    for (void *p : adj)
+        if (p) cudaFree(p);
     if (s.offs) cudaFree(s.offs);
     s = Species{};
 }
@@ -112,6 +115,12 @@ int alloc_species(pic_ctx *c, int kind, int64_t cap, bool spin) {
     }
     r = r ? r : dalloc(c, &s.d_count, sizeof(long long));
     if (c->p.adjoint && cap > 0) r = r ? r : dalloc(c, &s.dead, n);
+    if (c->p.adjoint && c->tile > 0 && cap > 0) {
+        r = r ? r : dalloc(c, &s.orig, n * sizeof(int));
+        r = r ? r : dalloc(c, &s.orig_b, n * sizeof(int));
+        r = r ? r : dalloc(c, &s.dead_b, n);
+        r = r ? r : dalloc(c, &s.perm, n * sizeof(int));
+    }
     if (r != PIC_OK) {
         free_species(s);
         return r;
@@ -243,6 +252,7 @@ int begin_fill(pic_ctx *c, int kind, int64_t n, bool spin_nonzero, double wmax) 
     }
     s.cur = 0;
     s.sorted = false;
+    s.perm_fresh = false;
     if (s.dead) cudaMemsetAsync(s.dead, 0, (size_t)s.cap, c->stream);
     s.spin_nonzero = spin_nonzero;
     s.max_abs_w = wmax;
@@ -254,6 +264,7 @@ int end_fill(pic_ctx *c, int kind, int64_t n, const char *what) {
     Species &s = c->sp[kind];
     long long cnt = n;
     CK(cudaMemcpyAsync(s.d_count, &cnt, sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+    if (s.orig && n > 0) launch_iota(c, s.orig, n);   // upload index of every particle
     CK(cudaStreamSynchronize(c->stream));
     s.n_host = n;
     int r = ensure_lists(c, n > c->sp[1 - kind].cap ? n : c->sp[1 - kind].cap);
@@ -384,12 +395,11 @@ int pic_create(const PicParams *pp, int device, pic_ctx **out) {
     // tiling: 0 -> default edge of 4 cells, < 0 -> global-memory kernel only
     c->tile = p.tile == 0 ? 4 : (p.tile < 0 ? 0 : p.tile);
     if (p.adjoint) {
-        // per-particle adjoints need particle indices that never change:
-        // no sorting, removal only marks particles dead
+        // removal only marks particles dead (no compaction); the counting
+        // sort still runs, recording each permutation for the reverse sweep
         if (p.rank_period[0] || p.rank_period[1] || p.rank_period[2])
             return bad("the adjoint supports absorbing faces only");
         if (p.absorbing) return bad("the adjoint has no transpose of the absorbing-faces extension");
-        c->tile = 0;
     }
     c->sort_interval = p.sort_interval > 0 ? p.sort_interval : 4;
     if (c->tile > 0) {
@@ -888,6 +898,7 @@ int pic_eval(pic_ctx *c, int what, const double *in, int nin, double *out, int n
 int pic_initial_push(pic_ctx *c) {
     if (!c) return PIC_EINVAL;
     int r;
+    launch_sort_due(c, 3);   // before the tape records the particles: the push runs in sorted order
     adjoint_record_hook(c);
     if ((r = push_both(c))) return r;
     if ((r = pic_exchange_particles(c, 0))) return r;
@@ -904,6 +915,7 @@ static int run_one_step(pic_ctx *c, bool rho_observed) {
     if ((r = pic_radiating_boundary(c, 1, 0, c->step))) return r;
     if ((r = pic_update_fields_first(c))) return r;
     if ((r = pic_clear_currents(c))) return r;
+    launch_sort_due(c, 3);
     adjoint_record_hook(c);
     if ((r = push_both(c))) return r;
     if ((r = pic_exchange_particles(c, 0))) return r;

@@ -116,6 +116,13 @@ struct Species {
     int *keys = nullptr;     // per-particle sort key
     int *strag = nullptr;    // particles the tiled kernel hands to the global kernel
     unsigned char *dead = nullptr;  // adjoint mode: 1 once a particle left through an absorbing face
+    // adjoint mode with tiles: the sort moves every per-particle array, so
+    // the upload index travels with the particle (orig) and each sort's
+    // gather permutation (perm[new] = old) is kept for the tape
+    int *orig = nullptr, *orig_b = nullptr;
+    unsigned char *dead_b = nullptr;
+    int *perm = nullptr;
+    bool perm_fresh = false;   // perm holds a sort the tape has not recorded yet
     unsigned *offs = nullptr;  // per-key start offsets after the last sort (nkeys + 1)
     bool sorted = false;     // offs describes the current order
     int pushes_since_sort = 0;

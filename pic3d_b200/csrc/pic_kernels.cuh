@@ -47,10 +47,12 @@ void launch_upload_particles(pic_ctx *c, int kind, const void *d_records, int64_
                              unsigned long long *check = nullptr);
 void launch_download_particles(pic_ctx *c, int kind, void *d_records, int64_t n, int64_t offset);
 void launch_convert_array(pic_ctx *c, void *dst, const void *src, long long n, int to_device);
+void launch_iota(pic_ctx *c, int *a, long long n);   // a[i] = i
 void launch_deposit_one(pic_ctx *c, int kind, const double (&xo)[3], const double (&xn)[3], double qw);
 
 // tile_kernels.cu
 void launch_sort(pic_ctx *c, int kind);
+void launch_sort_due(pic_ctx *c, int mask);   // the sorts the next push of the masked species needs
 void launch_tile_push(pic_ctx *c, int mask);
 size_t tile_smem_bytes(const pic_ctx *c);
 

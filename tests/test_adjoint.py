@@ -145,3 +145,41 @@ def test_autograd_function():
     _, gk, gp, _ = objective_and_grad(spec, knots, prof)
     np.testing.assert_allclose(kt.grad.numpy(), 2.0 * gk, rtol=1e-9)
     np.testing.assert_allclose(pt.grad.numpy(), 2.0 * gp, rtol=1e-9)
+
+
+def test_differentiable_run_gradient_matches_fd_on_8_parameters():
+    """The differentiable-run configuration (64x64x128, 8 electrons per cell,
+    32 density knots, 8x8 laser coefficients, 600 steps, checkpoints every
+    50): the FP64 adjoint gradient against central differences of the FP64
+    objective on the 4 knots and the 4 laser coefficients with the largest
+    derivatives.  The objective is piecewise smooth (electrons removed at the
+    absorbing faces are jumps), so the difference quotient converges only
+    once the step is too small to move a removal to another step; the check
+    takes the best of three relative steps and requires 1e-4."""
+    from pic3d_b200 import workloads as W
+    from pic3d_b200.adjoint import AdjointSpec, objective, objective_and_grad
+    w = W.differentiable_laser(precision="fp64", steps=600)
+    spec = AdjointSpec(workload=w, n_knots=32, profile_n=8, window=(0.5 * w.nx, w.nx - 4.0), ramp=4.0,
+                       segment=50, seed=2468, precision="fp64")
+    rng = np.random.default_rng(13)
+    knots = 0.01 + 0.02 * rng.random(32)
+    prof = 1.0 + 0.2 * rng.random((8, 8))
+    _, gk, gp, _ = objective_and_grad(spec, knots, prof)
+    checks = [("knot", int(i)) for i in np.argsort(-np.abs(gk))[:4]] + \
+             [("prof", int(i)) for i in np.argsort(-np.abs(gp))[:4]]
+    for which, i in checks:
+        g = gk[i] if which == "knot" else gp[i]
+        base = knots[i] if which == "knot" else prof.ravel()[i]
+        errs = []
+        for rel_h in (1e-7, 1e-8, 1e-9):
+            h = rel_h * abs(base)
+            k1, k2, p1, p2 = knots.copy(), knots.copy(), prof.ravel().copy(), prof.ravel().copy()
+            if which == "knot":
+                k1[i] += h
+                k2[i] -= h
+            else:
+                p1[i] += h
+                p2[i] -= h
+            f = (objective(spec, k1, p1) - objective(spec, k2, p2)) / (2 * h)
+            errs.append(abs(g - f) / max(abs(f), 1e-300))
+        assert min(errs) <= 1e-4, (which, i, g, errs)
