@@ -289,13 +289,13 @@ def fp32_error_bench(local, steps=200, samples=(1, 2, 5, 10, 20, 50, 100, 200)):
     return out
 
 
-def laser_bench(local, rank, warmup_steps, steps, precision):
+def laser_bench(local, rank, warmup_steps, steps, precision, cells=(256, 128, 128)):
     """The laser-in-underdense-plasma configuration (256x128x128, 4th order,
     8 + 8 particles per cell, a0 = 2, absorbing), timed after `warmup_steps`
     steps so that the pulse is inside the plasma and electrons move."""
     from pic3d_b200 import workloads as W
     from pic3d_b200.simulation import Simulation
-    w = W.laser_underdense(precision=precision)
+    w = W.laser_underdense(nx=cells[0], ny=cells[1], nz=cells[2], precision=precision)
     parts = W.make_particles(w, seed=1234 + rank)
     sim = Simulation(w, precision=precision, device=local, **TILE)
     for k in range(2):
@@ -480,23 +480,47 @@ def adjoint_bench(steps=600, short_steps=100):
     knots = 0.01 + 0.02 * rng.random(32)
     prof = 1.0 + 0.2 * rng.random((8, 8))
 
-    def grad(sp):
+    def grad(sp, kernels=False):
         run = AdjointRun(sp, knots, prof)
         run.sim.synchronize()
         t0 = time.perf_counter()
         loss = run.forward()
         run.sim.synchronize()
         t1 = time.perf_counter()
+        if kernels:
+            run.sim.profile(True)
+            run.sim.profile_reset()
         gw, gp = run.backward()
         run.sim.synchronize()
         t2 = time.perf_counter()
+        kern = run.sim.profile_read() if kernels else {}
         gk = sp.knot_grad(run.x0, gw)
         n = len(run.records)
         run.close()
-        return dict(loss=loss, gk=gk, gp=gp, fwd=t1 - t0, bwd=t2 - t1, n=n)
+        return dict(loss=loss, gk=gk, gp=gp, fwd=t1 - t0, bwd=t2 - t1, n=n,
+                    kernels={k: {"ms_total": v[0], "launches": v[1]} for k, v in kern.items()})
+
+    def production_forward(sp):
+        """The same run (particles, weights, laser) in an ordinary context:
+        the forward cost a user pays without the adjoint."""
+        from pic3d_b200.simulation import Simulation
+        rec = sp.base_particles()
+        rec["weight"] = sp.weights(rec["x"].copy(), knots)
+        sim = Simulation(sp.workload, precision=sp.precision, laser_profile=prof.reshape(8, 8), **TILE)
+        sim.upload_particles(0, rec)
+        sim.upload_particles(1, np.zeros(0, rec.dtype))
+        sim.synchronize()
+        t0 = time.perf_counter()
+        sim.initial_push()
+        sim.run_main_time_loop(sp.workload.steps)
+        sim.synchronize()
+        dt = time.perf_counter() - t0
+        sim.close()
+        return dt
 
     rel = lambda x, y: float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
-    a, b = grad(spec("fp32")), grad(spec("fp64"))
+    a, b = grad(spec("fp32"), kernels=True), grad(spec("fp64"))
+    prod32 = production_forward(spec("fp32"))
     sa, sb = grad(spec("fp32", short_steps)), grad(spec("fp64", short_steps))
     sp64 = spec("fp64")
     checks = []
@@ -521,15 +545,18 @@ def adjoint_bench(steps=600, short_steps=100):
                                                   "sin^2 ramps",
             "objective_fp32": a["loss"], "objective_fp64": b["loss"],
             "forward_s": a["fwd"], "adjoint_s": a["bwd"], "adjoint_over_forward": a["bwd"] / a["fwd"],
+            "production_forward_s": prod32, "adjoint_over_production_forward": a["bwd"] / prod32,
+            "adjoint_kernels_fp32": a["kernels"],
             "fp64_forward_s": b["fwd"], "fp64_adjoint_s": b["bwd"],
             "grad_rel_l2_fp32_vs_fp64": {"knots": rel(a["gk"], b["gk"]), "laser": rel(a["gp"], b["gp"])},
             f"grad_rel_l2_fp32_vs_fp64_{short_steps}_steps": {"knots": rel(sa["gk"], sb["gk"]),
                                                               "laser": rel(sa["gp"], sb["gp"])},
             "finite_difference_checks": checks,
             "note": "adjoint = restore each checkpoint, recompute its 50 steps recording the push inputs, reverse "
-                    "sweep; forward = the run with checkpoints; both in adjoint mode (global push kernel); central "
-                    "differences of a piecewise-smooth objective converge only at small steps (particle removal "
-                    "at the absorbing faces)"}
+                    "sweep; forward = the run with checkpoints in the adjoint-capable context (tiled push, sorts "
+                    "recorded); production forward = the same run in an ordinary context; central differences of a "
+                    "piecewise-smooth objective converge only at small steps (particle removal at the absorbing "
+                    "faces)"}
 
 
 def main():
@@ -547,6 +574,8 @@ def main():
     ap.add_argument("--no-fp32-error", action="store_true")
     ap.add_argument("--no-laser", action="store_true")
     ap.add_argument("--laser-warmup", type=int, default=600)
+    ap.add_argument("--laser-cells", default="256,128,128", help="laser grid (smaller grids for profiling)")
+    ap.add_argument("--laser-only", action="store_true", help="only the laser configuration (profiling)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--adjoint-steps", type=int, default=600)
@@ -573,6 +602,12 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
+    if args.laser_only:
+        lc = tuple(int(v) for v in args.laser_cells.split(","))
+        out = laser_bench(local, rank, args.laser_warmup, args.steps, args.precision, lc)
+        if rank == 0:
+            print(json.dumps({"laser": out}), flush=True)
+        return
     nx, ny, nz = (int(v) for v in args.cells.split(","))
     mem, prec = (2 if args.order == 2 else 4), args.precision
     w, sim = thermal_sim(mem, prec, local, 97 + 2 * rank, nx, ny, nz)

@@ -46,6 +46,7 @@ class AdjointSpec:
     segment: int = 50
     seed: int = 4321
     precision: str = "fp32"
+    tile: int = 0                     # particle tile edge (0 default; -1 global-memory kernels, unsorted)
 
     def base_particles(self):
         """Electron positions and momenta (weights set from the knots)."""
@@ -73,7 +74,7 @@ class AdjointRun:
 
     def __init__(self, spec: AdjointSpec, knots, profile, device: int = 0):
         self.spec = spec
-        self.sim = Simulation(spec.workload, precision=spec.precision, device=device, adjoint=True,
+        self.sim = Simulation(spec.workload, precision=spec.precision, device=device, adjoint=True, tile=spec.tile,
                               laser_profile=np.asarray(profile, dtype=np.float64).reshape(spec.profile_n,
                                                                                            spec.profile_n))
         rec = spec.base_particles()

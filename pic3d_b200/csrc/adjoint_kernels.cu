@@ -155,8 +155,8 @@ __device__ __forceinline__ void shape_derivs(real d, real (&w)[5]) {
 }
 
 // gather of one component with its gradient with respect to the position
-template <typename real, int P>
-__device__ __forceinline__ void gather_grad(const real *f, const Geom &g, int i0, int j0, int k0,
+template <typename real, int P, bool LDG>
+__device__ __forceinline__ void gather_grad(const View<const real> &f, int i0, int j0, int k0,
                                             const real (&wx)[P], const real (&wy)[P], const real (&wz)[P],
                                             const real (&dx)[P], const real (&dy)[P], const real (&dz)[P], real &e,
                                             real (&gr)[3]) {
@@ -166,11 +166,11 @@ __device__ __forceinline__ void gather_grad(const real *f, const Geom &g, int i0
         real a = 0, ax = 0, ay = 0;
 #pragma unroll
         for (int j = 0; j < P; ++j) {
-            const real *row = f + g.fi(k0 + k, j0 + j, i0);
+            const real *row = f.at(k0 + k, j0 + j, i0);
             real s = 0, sd = 0;
 #pragma unroll
             for (int i = 0; i < P; ++i) {
-                real v = __ldg(row + i);
+                real v = LDG ? __ldg(row + i) : row[i];
                 s += wx[i] * v;
                 sd += dx[i] * v;
             }
@@ -220,7 +220,7 @@ __device__ __forceinline__ void span_pair(int i1, const T (&a0)[P], int i2, cons
 // ds = s1 - s0, axes `u` and `v` the weight
 // W = 1/3 s0u s0v + 1/6 s1u s0v + 1/6 s0u s1v + 1/3 s1u s1v.
 // Returns G1 = sum(lam * J) / w and adds dG1/ds0, dG1/ds1 into g0, g1.
-template <int P, typename LT>
+template <int P, bool LDG, typename LT>
 __device__ __forceinline__ double esirkepov_adj(const LT *lam, int sc, int su, int sv, int lc, int lu, int lv,
                                                 double coef, const double (&s0c)[P + 1], const double (&s1c)[P + 1],
                                                 const double (&s0u)[P + 1], const double (&s1u)[P + 1],
@@ -251,7 +251,7 @@ __device__ __forceinline__ double esirkepov_adj(const LT *lam, int sc, int su, i
 #pragma unroll
             for (int q = 0; q < P; ++q) {
                 if (q >= lc - 1) break;
-                const double l = (double)__ldg(row + q * sc);
+                const double l = (double)(LDG ? __ldg(row + q * sc) : row[q * sc]);
                 T += C[q] * l;
                 M[q] += l * W;
             }
@@ -303,16 +303,24 @@ struct AdjPushArgs {
     double d_dt[3];
     int scatter_fields;        // 0 for the t = 0 push (fields identically zero there)
     unsigned *status;
+    const int *idx;            // optional particle list (count *nidx); null: all n particles
+    const unsigned long long *nidx;
 };
 
-template <typename real, int P>
-__global__ void __launch_bounds__(128) adj_push_kernel(AdjPushArgs<real> a) {
+// One particle's push adjoint (everything but the scatter of the gathered
+// field adjoints): per-particle adjoints updated in place, the weight
+// adjoint accumulated, and lin[3..8] = d objective / d(gathered E, B) left
+// for the caller to scatter with the gather weights.  fv: the tape's six
+// field components; lj: the three J adjoints (ring layout or a shared box),
+// both addressed in buffer coordinates.  Returns false if the particle is
+// skipped (its stencil leaves the buffers).
+template <typename real, int P, bool LDG>
+__device__ __forceinline__ bool adj_particle(const AdjPushArgs<real> &a, long long p, const View<const real> (&fv)[6],
+                                             const View<const real> (&lj)[3], real (&lin)[9]) {
     constexpr bool F64 = sizeof(real) == 8;
     constexpr int H = P / 2;
     const Geom &g = a.g;
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n;
-         p += (long long)gridDim.x * blockDim.x) {
-        if (a.dead && a.dead[p]) continue;
+    {
         // ---- old position --------------------------------------------------
         int ip[3], id[3], cc[3] = {0, 0, 0};
         real dp[3], dd[3];
@@ -350,7 +358,7 @@ __global__ void __launch_bounds__(128) adj_push_kernel(AdjPushArgs<real> a) {
         for (int d = 0; d < 3; ++d) ok = ok && id[d] >= H && ip[d] <= g.f[d] - 1 - H;
         if (!ok) {
             set_status(a.status, ST_OOB);
-            continue;
+            return false;
         }
         // ---- gather with gradients (Yee staggering, particle.cpp:207-259) -
         real ev[6], eg[6][3];
@@ -363,12 +371,12 @@ __global__ void __launch_bounds__(128) adj_push_kernel(AdjPushArgs<real> a) {
             shape_derivs(dp[d], gp[d]);
             shape_derivs(dd[d], gd[d]);
         }
-        gather_grad<real, P>(a.f[0], g, id[0] - H, ip[1] - H, ip[2] - H, wd[0], wp[1], wp[2], gd[0], gp[1], gp[2], ev[0], eg[0]);
-        gather_grad<real, P>(a.f[1], g, ip[0] - H, id[1] - H, ip[2] - H, wp[0], wd[1], wp[2], gp[0], gd[1], gp[2], ev[1], eg[1]);
-        gather_grad<real, P>(a.f[2], g, ip[0] - H, ip[1] - H, id[2] - H, wp[0], wp[1], wd[2], gp[0], gp[1], gd[2], ev[2], eg[2]);
-        gather_grad<real, P>(a.f[3], g, ip[0] - H, id[1] - H, id[2] - H, wp[0], wd[1], wd[2], gp[0], gd[1], gd[2], ev[3], eg[3]);
-        gather_grad<real, P>(a.f[4], g, id[0] - H, ip[1] - H, id[2] - H, wd[0], wp[1], wd[2], gd[0], gp[1], gd[2], ev[4], eg[4]);
-        gather_grad<real, P>(a.f[5], g, id[0] - H, id[1] - H, ip[2] - H, wd[0], wd[1], wp[2], gd[0], gd[1], gp[2], ev[5], eg[5]);
+        gather_grad<real, P, LDG>(fv[0], id[0] - H, ip[1] - H, ip[2] - H, wd[0], wp[1], wp[2], gd[0], gp[1], gp[2], ev[0], eg[0]);
+        gather_grad<real, P, LDG>(fv[1], ip[0] - H, id[1] - H, ip[2] - H, wp[0], wd[1], wp[2], gp[0], gd[1], gp[2], ev[1], eg[1]);
+        gather_grad<real, P, LDG>(fv[2], ip[0] - H, ip[1] - H, id[2] - H, wp[0], wp[1], wd[2], gp[0], gp[1], gd[2], ev[2], eg[2]);
+        gather_grad<real, P, LDG>(fv[3], ip[0] - H, id[1] - H, id[2] - H, wp[0], wd[1], wd[2], gp[0], gd[1], gd[2], ev[3], eg[3]);
+        gather_grad<real, P, LDG>(fv[4], id[0] - H, ip[1] - H, id[2] - H, wd[0], wp[1], wd[2], gd[0], gp[1], gd[2], ev[4], eg[4]);
+        gather_grad<real, P, LDG>(fv[5], id[0] - H, id[1] - H, ip[2] - H, wd[0], wd[1], wp[2], gd[0], gd[1], gp[2], ev[5], eg[5]);
         }
         // ---- Boris Jacobian: three passes of three tangents (p, e, b) -----
         const real pin[3] = {a.px[p], a.py[p], a.pz[p]};
@@ -411,7 +419,7 @@ __global__ void __launch_bounds__(128) adj_push_kernel(AdjPushArgs<real> a) {
         bool cfl = abs(i2[0] - ip[0]) <= 1 && abs(i2[1] - ip[1]) <= 1 && abs(i2[2] - ip[2]) <= 1;
         if (!cfl) {
             set_status(a.status, ST_CFL);
-            continue;
+            return false;
         }
         // ---- deposit adjoint ----------------------------------------------
         double s0[3][P + 1], s1[3][P + 1];   // weights on the common span
@@ -434,16 +442,16 @@ __global__ void __launch_bounds__(128) adj_push_kernel(AdjPushArgs<real> a) {
         // the J adjoints are read in place from the ring buffers
 #pragma unroll 1
         for (int comp = 0; comp < 3; ++comp) {
-            const real *lbuf = a.lj[comp] + g.ri(base[2], base[1], base[0]);
-            const int sX = 1, sY = g.r[0], sZ = g.rxy;
+            const real *lbuf = lj[comp].at(base[2], base[1], base[0]);
+            const int sX = 1, sY = lj[comp].sy, sZ = lj[comp].sz;
             if (comp == 0)
-                G1 += esirkepov_adj<P>(lbuf, sX, sY, sZ, len[0], len[1], len[2], -qd * a.d_dt[0], s0[0], s1[0],
+                G1 += esirkepov_adj<P, LDG>(lbuf, sX, sY, sZ, len[0], len[1], len[2], -qd * a.d_dt[0], s0[0], s1[0],
                                        s0[1], s1[1], s0[2], s1[2], g0[0], g1[0], g0[1], g1[1], g0[2], g1[2]);
             else if (comp == 1)
-                G1 += esirkepov_adj<P>(lbuf, sY, sX, sZ, len[1], len[0], len[2], -qd * a.d_dt[1], s0[1], s1[1],
+                G1 += esirkepov_adj<P, LDG>(lbuf, sY, sX, sZ, len[1], len[0], len[2], -qd * a.d_dt[1], s0[1], s1[1],
                                        s0[0], s1[0], s0[2], s1[2], g0[1], g1[1], g0[0], g1[0], g0[2], g1[2]);
             else
-                G1 += esirkepov_adj<P>(lbuf, sZ, sX, sY, len[2], len[0], len[1], -qd * a.d_dt[2], s0[2], s1[2],
+                G1 += esirkepov_adj<P, LDG>(lbuf, sZ, sX, sY, len[2], len[0], len[1], -qd * a.d_dt[2], s0[2], s1[2],
                                        s0[0], s1[0], s0[1], s1[1], g0[2], g1[2], g0[0], g1[0], g0[1], g1[1]);
         }
         const double wgt = (double)a.w[p];
@@ -468,7 +476,6 @@ __global__ void __launch_bounds__(128) adj_push_kernel(AdjPushArgs<real> a) {
         // b), one forward-mode pass of three tangents per input group ------
         const real lxn[3] = {a.lx[p] + (real)dGx1[0], a.ly[p] + (real)dGx1[1], a.lz[p] + (real)dGx1[2]};
         const real lpn[3] = {a.lpx[p], a.lpy[p], a.lpz[p]};
-        real lin[9];
 #pragma unroll
         for (int pass = 0; pass < 3; ++pass) {
             Dual<real, 3> P_[3], E_[3], B_[3], pn[3], ds[3];
@@ -507,13 +514,62 @@ __global__ void __launch_bounds__(128) adj_push_kernel(AdjPushArgs<real> a) {
         a.lpx[p] = lin[0];
         a.lpy[p] = lin[1];
         a.lpz[p] = lin[2];
-        if (a.scatter_fields) {
-            real wp[3][P], wd[3][P];   // the gather weights again (cheaper than keeping them live)
+        return true;
+    }
+}
+
+// The gather weights of the six staggered components of a particle at its
+// tape position (primal/dual index and offset per axis), for the scatter.
+template <typename real, int P>
+__device__ __forceinline__ void gather_stencils(const AdjPushArgs<real> &a, long long p, int (&ip)[3], int (&id)[3],
+                                                real (&wp)[3][P], real (&wd)[3][P]) {
+    const Geom &g = a.g;
+    if constexpr (sizeof(real) == 8) {
+        const double xd[3] = {a.x[p], a.y[p], a.z[p]};
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                shape_weights(dp[d], wp[d]);
-                shape_weights(dd[d], wd[d]);
-            }
+        for (int d = 0; d < 3; ++d) {
+            double xc = xd[d] - (double)(1 - g.mem);
+            ip[d] = (int)(xc + 0.5);
+            id[d] = (int)xc;
+            shape_weights((real)(xc - (double)ip[d]), wp[d]);
+            shape_weights((real)((xc - 0.5) - (double)id[d]), wd[d]);
+        }
+    } else {
+        int cc[3];
+        a.cp.unpack(a.cell[p], cc[0], cc[1], cc[2]);
+        const real oo[3] = {a.ox[p], a.oy[p], a.oz[p]};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const int b = cc[d] + g.mem - 1;
+            const bool up = oo[d] >= 0.5f;
+            ip[d] = b + (up ? 1 : 0);
+            id[d] = b;
+            shape_weights(up ? oo[d] - 1.0f : oo[d], wp[d]);
+            shape_weights(oo[d] - 0.5f, wd[d]);
+        }
+    }
+}
+
+template <typename real, int P>
+__global__ void __launch_bounds__(128) adj_push_kernel(AdjPushArgs<real> a) {
+    constexpr int H = P / 2;
+    const Geom &g = a.g;
+    View<const real> fv[6], lj[3];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) fv[c] = View<const real>{a.f[c], g.f[0], g.fxy, 0};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) lj[c] = View<const real>{a.lj[c], g.r[0], g.rxy, g.rxy + g.r[0] + 1};
+    const long long n = a.idx ? (long long)*a.nidx : a.n;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long p = a.idx ? (long long)a.idx[t] : t;
+        if (a.dead && a.dead[p]) continue;
+        real lin[9];
+        if (!adj_particle<real, P, true>(a, p, fv, lj, lin)) continue;
+        if (a.scatter_fields) {
+            int ip[3], id[3];
+            real wp[3][P], wd[3][P];   // the gather weights again (cheaper than keeping them live)
+            gather_stencils<real, P>(a, p, ip, id, wp, wd);
             scatter_adj<real, P>(a.lf[0], g, id[0] - H, ip[1] - H, ip[2] - H, wd[0], wp[1], wp[2], lin[3]);
             scatter_adj<real, P>(a.lf[1], g, ip[0] - H, id[1] - H, ip[2] - H, wp[0], wd[1], wp[2], lin[4]);
             scatter_adj<real, P>(a.lf[2], g, ip[0] - H, ip[1] - H, id[2] - H, wp[0], wp[1], wd[2], lin[5]);
@@ -522,6 +578,208 @@ __global__ void __launch_bounds__(128) adj_push_kernel(AdjPushArgs<real> a) {
             scatter_adj<real, P>(a.lf[5], g, id[0] - H, id[1] - H, ip[2] - H, wd[0], wd[1], wp[2], lin[8]);
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Tiled push adjoint.  The tape holds the particles in the order of the
+// forward push, i.e. sorted by tile at the last sort; with each sort the tape
+// also keeps the tile boundaries of that order.  One CTA per tile:
+//   1. stages the tape's six field components over the tile's gather box
+//      and the three J adjoints over its deposit box in shared memory;
+//   2. runs each particle's push adjoint from shared memory, keeping the
+//      adjoints of its gathered E and B (six values) and their largest
+//      magnitude per component;
+//   3. adds every particle's field adjoint times its gather weights into
+//      fixed-point shared accumulators (20-bit limbs as the forward deposit,
+//      scaled so that the largest value fits), then flushes them with one
+//      pass of global atomics.
+// Particles that left their tile since the sort, and tiles with more
+// particles than the scratch holds, go to the global kernel afterwards.
+
+struct AdjTileGeom {
+    int T, nt[3];
+    int GE, DE;
+    int gsy, gsz, gsize, dsy, dsz, dsize;
+    int cap;                 // particles per tile the shared scratch holds
+};
+
+template <typename real>
+constexpr int adj_limbs() { return sizeof(real) == 8 ? 3 : 2; }
+
+template <typename real, int NL>
+__device__ __forceinline__ void fixed_add(unsigned *a, int lstride, real q) {
+    if (q == real(0)) return;
+    if constexpr (NL == 3) {
+        const long long qi = __double_as_longlong((double)q + 6755399441055744.0) - 0x4338000000000000LL;
+        atomicAdd(a, (unsigned)(qi & 0xFFFFF));
+        atomicAdd(a + lstride, (unsigned)((qi >> 20) & 0xFFFFF));
+        atomicAdd(a + 2 * lstride, (unsigned)(int)(qi >> 40));
+    } else {
+        const int qi = __float2int_rn((float)q);
+        atomicAdd(a, (unsigned)qi & 0xFFFFFu);
+        atomicAdd(a + lstride, (unsigned)(qi >> 20));
+    }
+}
+
+template <typename real, int P>
+__global__ void __launch_bounds__(256, 1) adj_tile_kernel(AdjPushArgs<real> a, AdjTileGeom t, const unsigned *toffs,
+                                                          int *strag, unsigned long long *nstrag) {
+    constexpr int H = P / 2, NL = adj_limbs<real>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Geom &g = a.g;
+    const int T = t.T, GE = t.GE, DE = t.DE, GS = t.gsize, DS = t.dsize;
+    real *sf = reinterpret_cast<real *>(smem_raw);              // 6 x GS
+    real *sl = sf + 6 * GS;                                       // 3 x DS
+    real *slin = sl + 3 * DS;                                     // cap x 6
+    unsigned *acc = reinterpret_cast<unsigned *>(slin + 6 * t.cap);   // 6 x NL x GS
+    unsigned *smax = acc + 6 * NL * GS;                           // 6 (bits of non-negative values)
+    unsigned char *flag = reinterpret_cast<unsigned char *>(smax + 8);   // cap
+    const int tile = blockIdx.x;
+    const int tx = tile % t.nt[0], ty = (tile / t.nt[0]) % t.nt[1], tz = tile / (t.nt[0] * t.nt[1]);
+    const int t0[3] = {tx * T, ty * T, tz * T};
+    int gO[3], dO[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        gO[d] = t0[d] + g.mem - 1 - H;
+        dO[d] = t0[d] + g.mem - 2 - H;
+    }
+    long long pa = toffs[tile], pb = toffs[tile + 1];
+    pb = pb < a.n ? pb : a.n;
+    if (pa > pb) pa = pb;
+    const long long m = pb - pa;
+    if (m == 0) return;
+    const bool use_smem = m <= t.cap;
+    if (!use_smem) {
+        for (long long i = threadIdx.x; i < m; i += blockDim.x) {
+            const long long p = pa + i;
+            if (!(a.dead && a.dead[p])) strag[atomicAdd(nstrag, 1ull)] = (int)p;
+        }
+        return;
+    }
+    const int G2 = GE * GE, G3 = G2 * GE, D2 = DE * DE, D3 = D2 * DE;
+    for (int e = threadIdx.x; e < 6 * G3; e += blockDim.x) {
+        int c = e / G3, l = e - c * G3;
+        int lz = l / G2, r = l - lz * G2, ly = r / GE, lx = r - ly * GE;
+        int x = gO[0] + lx, y = gO[1] + ly, z = gO[2] + lz;
+        real v = 0;
+        if (x >= 0 && x < g.f[0] && y >= 0 && y < g.f[1] && z >= 0 && z < g.f[2]) v = __ldg(a.f[c] + g.fi(z, y, x));
+        sf[c * GS + lz * t.gsz + ly * t.gsy + lx] = v;
+    }
+    for (int e = threadIdx.x; e < 3 * D3; e += blockDim.x) {
+        int c = e / D3, l = e - c * D3;
+        int lz = l / D2, r = l - lz * D2, ly = r / DE, lx = r - ly * DE;
+        int x = dO[0] + lx, y = dO[1] + ly, z = dO[2] + lz;
+        real v = 0;
+        if (x >= -1 && x <= g.f[0] && y >= -1 && y <= g.f[1] && z >= -1 && z <= g.f[2]) v = __ldg(a.lj[c] + g.ri(z, y, x));
+        sl[c * DS + lz * t.dsz + ly * t.dsy + lx] = v;
+    }
+    for (int e = threadIdx.x; e < 6 * NL * GS; e += blockDim.x) acc[e] = 0u;
+    if (threadIdx.x < 6) smax[threadIdx.x] = 0u;
+    __syncthreads();
+    View<const real> fv[6], lj[3];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) fv[c] = View<const real>{sf + c * GS, t.gsy, t.gsz, -(gO[2] * t.gsz + gO[1] * t.gsy + gO[0])};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) lj[c] = View<const real>{sl + c * DS, t.dsy, t.dsz, -(dO[2] * t.dsz + dO[1] * t.dsy + dO[0])};
+    // 2. the particles' push adjoints
+    for (long long i = threadIdx.x; i < m; i += blockDim.x) {
+        const long long p = pa + i;
+        flag[i] = 0;
+        if (a.dead && a.dead[p]) continue;
+        int idl[3];   // dual index per axis (the cell's lower primal point)
+        if constexpr (sizeof(real) == 8) {
+            idl[0] = (int)(a.x[p] - (double)(1 - g.mem));
+            idl[1] = (int)(a.y[p] - (double)(1 - g.mem));
+            idl[2] = (int)(a.z[p] - (double)(1 - g.mem));
+        } else {
+            int cc[3];
+            a.cp.unpack(a.cell[p], cc[0], cc[1], cc[2]);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) idl[d] = cc[d] + g.mem - 1;
+        }
+        bool inside = true;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) inside = inside && idl[d] >= t0[d] + g.mem - 1 && idl[d] < t0[d] + g.mem - 1 + T;
+        if (!inside) {
+            strag[atomicAdd(nstrag, 1ull)] = (int)p;
+            continue;
+        }
+        real lin[9];
+        if (!adj_particle<real, P, false>(a, p, fv, lj, lin)) continue;
+        if (!a.scatter_fields) continue;
+        flag[i] = 1;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            slin[i * 6 + c] = lin[3 + c];
+            const float mag = (float)fabs(lin[3 + c]);
+            atomicMax(smax + c, __float_as_uint(mag));
+        }
+    }
+    if (!a.scatter_fields) return;
+    __syncthreads();
+    // 3. field adjoints into fixed point, then one flush
+    const double lim = sizeof(real) == 8 ? 2251799813685248.0 /* 2^51 */ : 2147483648.0 /* 2^31 */;
+    real scale[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        const double mx = (double)__uint_as_float(smax[c]);
+        scale[c] = mx > 0.0 ? (real)(lim / (1.01 * mx)) : real(0);
+    }
+    for (long long i = threadIdx.x; i < m; i += blockDim.x) {
+        if (!flag[i]) continue;
+        int ip[3], id[3];
+        real wp[3][P], wd[3][P];
+        gather_stencils<real, P>(a, pa + i, ip, id, wp, wd);
+        // stencil origin per component (Yee staggering as in the gather)
+        const int o[6][3] = {{id[0], ip[1], ip[2]}, {ip[0], id[1], ip[2]}, {ip[0], ip[1], id[2]},
+                             {ip[0], id[1], id[2]}, {id[0], ip[1], id[2]}, {id[0], id[1], ip[2]}};
+#pragma unroll 1
+        for (int c = 0; c < 6; ++c) {
+            const real q = slin[i * 6 + c] * scale[c];
+            if (q == real(0)) continue;
+            // dual axes: Ex x; Ey y; Ez z; Bx y, z; By x, z; Bz x, y
+            const bool dx_ = c == 0 || c == 4 || c == 5, dy_ = c == 1 || c == 3 || c == 5,
+                       dz_ = c == 2 || c == 3 || c == 4;
+            real wx[P], wy[P], wz[P];
+#pragma unroll
+            for (int q2 = 0; q2 < P; ++q2) {
+                wx[q2] = dx_ ? wd[0][q2] : wp[0][q2];
+                wy[q2] = dy_ ? wd[1][q2] : wp[1][q2];
+                wz[q2] = dz_ ? wd[2][q2] : wp[2][q2];
+            }
+            unsigned *ac = acc + c * NL * GS;
+            const int b0 = (o[c][2] - H - gO[2]) * t.gsz + (o[c][1] - H - gO[1]) * t.gsy + (o[c][0] - H - gO[0]);
+#pragma unroll 1
+            for (int k = 0; k < P; ++k) {
+                const real qk = q * pick(wz, k);
+#pragma unroll
+                for (int j = 0; j < P; ++j) {
+                    const real qj = qk * wy[j];
+#pragma unroll
+                    for (int ii = 0; ii < P; ++ii) fixed_add<real, NL>(ac + b0 + k * t.gsz + j * t.gsy + ii, GS, qj * wx[ii]);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < 6 * G3; e += blockDim.x) {
+        int c = e / G3, l = e - c * G3;
+        if (scale[c] == real(0)) continue;
+        int lz = l / G2, r = l - lz * G2, ly = r / GE, lx = r - ly * GE;
+        const unsigned *q = acc + c * NL * GS + lz * t.gsz + ly * t.gsy + lx;
+        long long tot;
+        if constexpr (NL == 2) tot = ((long long)(int)q[GS] << 20) + (long long)q[0];
+        else tot = ((long long)(int)q[2 * GS] << 40) + ((long long)q[GS] << 20) + (long long)q[0];
+        if (tot == 0) continue;
+        int x = gO[0] + lx, y = gO[1] + ly, z = gO[2] + lz;
+        if (x >= 0 && x < g.f[0] && y >= 0 && y < g.f[1] && z >= 0 && z < g.f[2])
+            atomic_add(a.lf[c] + g.fi(z, y, x), (real)((double)tot / (double)scale[c]));
+    }
+}
+
+__global__ void tile_bounds_kernel(const unsigned *offs, long long keys_per_tile, int ntiles, unsigned *out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t <= ntiles) out[t] = offs[(long long)t * keys_per_tile];
 }
 
 // ---------------------------------------------------------------------------
@@ -740,6 +998,7 @@ struct Blob {
     long long count[2] = {0, 0};
     int field_part = 0;          // tape: index of the first of the six field parts
     int perm_part[2] = {-1, -1}; // tape: the sort permutation run right before this push, per species
+    int toff_part[2] = {-1, -1}; // tape: tile boundaries of the particle order of this push, per species
 };
 
 struct AdjState {
@@ -759,6 +1018,7 @@ struct AdjState {
     // per-particle adjoints are held in (valid once seeded), and scratch
     int *lam_orig[2] = {};
     bool lam_valid = false;
+    unsigned *toffs[2] = {};   // tiled contexts: tile boundaries extracted for the tape
     void *tmp = nullptr;
     size_t tmp_bytes = 0;
 };
@@ -861,7 +1121,7 @@ void adjoint_record_hook(pic_ctx *c) {
     particle_parts(c, parts);
     const int field_part = (int)parts.size();
     for (int f = 0; f < 6; ++f) parts.push_back({c->field[f], (size_t)c->g.fsz * rsize(c)});
-    int perm_part[2] = {-1, -1};
+    int perm_part[2] = {-1, -1}, toff_part[2] = {-1, -1};
     for (int k = 0; k < 2; ++k) {
         Species &s = c->sp[k];
         if (!s.perm_fresh || s.n_host == 0) continue;
@@ -869,12 +1129,23 @@ void adjoint_record_hook(pic_ctx *c) {
         parts.push_back({s.perm, (size_t)s.n_host * sizeof(int)});
         s.perm_fresh = false;
     }
+    const int ntiles = c->ntile[0] * c->ntile[1] * c->ntile[2];
+    for (int k = 0; k < 2; ++k) {
+        Species &s = c->sp[k];
+        if (c->tile <= 0 || s.n_host == 0 || !s.sorted || !A->toffs[k]) continue;
+        const long long kpt = (long long)c->tile * c->tile * c->tile * kOctants;
+        tile_bounds_kernel<<<(ntiles + 256) / 256, 256, 0, c->stream>>>(s.offs, kpt, ntiles, A->toffs[k]);
+        toff_part[k] = (int)parts.size();
+        parts.push_back({A->toffs[k], (size_t)(ntiles + 1) * sizeof(unsigned)});
+    }
     prof_begin(c, "adjoint_tape_record");
     Blob &b = A->tape[A->tape_len];
     if (blob_save(c, b, parts) == PIC_OK) {
         b.field_part = field_part;
         b.perm_part[0] = perm_part[0];
         b.perm_part[1] = perm_part[1];
+        b.toff_part[0] = toff_part[0];
+        b.toff_part[1] = toff_part[1];
         A->tape_len++;
     }
     prof_end(c);
@@ -1026,6 +1297,32 @@ static void adj_push_launch(pic_ctx *c, AdjState *A, const Blob &b, int kind, in
     a.scatter_fields = scatter;
     a.status = c->d_status;
     long long blocks = (a.n + 127) / 128;
+    if (c->tile > 0 && b.toff_part[kind] >= 0) {
+        // one CTA per tile, then the particles it handed back
+        const TileBoxes bx = tile_boxes(c);
+        AdjTileGeom tg{};
+        tg.T = c->tile;
+        for (int d = 0; d < 3; ++d) tg.nt[d] = c->ntile[d];
+        tg.GE = bx.GE; tg.DE = bx.DE;
+        tg.gsy = bx.gsy; tg.gsz = bx.gsz; tg.gsize = bx.gsize;
+        tg.dsy = bx.dsy; tg.dsz = bx.dsz; tg.dsize = bx.dsize;
+        const size_t rs = sizeof(real), nl = adj_limbs<real>();
+        const size_t fixed = (6 * (size_t)bx.gsize + 3 * (size_t)bx.dsize) * rs + (6 * nl * bx.gsize + 8) * 4;
+        const size_t budget = 227 * 1024;
+        tg.cap = fixed + 64 < budget ? (int)std::min<size_t>(4095, (budget - fixed - 64) / (6 * rs + 1)) : 0;
+        const size_t smem = fixed + (size_t)tg.cap * (6 * rs + 1);
+        const int ntiles = c->ntile[0] * c->ntile[1] * c->ntile[2];
+        cudaMemsetAsync(c->d_nstrag + kind, 0, sizeof(unsigned long long), c->stream);
+        prof_begin(c, "adjoint_tile_push_deposit");
+        if (tg.cap > 0) {
+            cudaFuncSetAttribute(adj_tile_kernel<real, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            adj_tile_kernel<real, P><<<ntiles, 256, smem, c->stream>>>(
+                a, tg, (const unsigned *)blob_part(b, b.toff_part[kind]), s.strag, c->d_nstrag + kind);
+            a.idx = s.strag;
+            a.nidx = c->d_nstrag + kind;
+        }
+        prof_end(c);
+    }
     prof_begin(c, "adjoint_push_deposit");
     adj_push_kernel<real, P><<<(unsigned)std::min<long long>(blocks, 148 * 16), 128, 0, c->stream>>>(a);
     prof_end(c);
@@ -1181,6 +1478,15 @@ int pic_adjoint_tape(pic_ctx *c, int nsteps) {
     AdjState *A = adj_of(c, true);
     if ((int)A->tape.size() < nsteps) A->tape.resize(nsteps);
     A->tape_len = 0;
+    if (c->tile > 0) {
+        const size_t nt = (size_t)c->ntile[0] * c->ntile[1] * c->ntile[2] + 1;
+        for (int k = 0; k < 2; ++k)
+            if (!A->toffs[k] && cudaMalloc((void **)&A->toffs[k], nt * sizeof(unsigned)) != cudaSuccess) {
+                A->toffs[k] = nullptr;
+                c->err = "adjoint: out of device memory for the tile boundaries";
+                return PIC_ENOMEM;
+            }
+    }
     return PIC_OK;
 }
 
@@ -1289,6 +1595,7 @@ int pic_adjoint_release(pic_ctx *c) {
         if (A->lprof) cudaFree(A->lprof);
         if (A->loss) cudaFree(A->loss);
         for (int *p : A->lam_orig) if (p) cudaFree(p);
+        for (unsigned *p : A->toffs) if (p) cudaFree(p);
         if (A->tmp) cudaFree(A->tmp);
         delete A;
         g_adj.erase(g_adj.begin() + (long)i);

@@ -54,6 +54,12 @@ void launch_deposit_one(pic_ctx *c, int kind, const double (&xo)[3], const doubl
 void launch_sort(pic_ctx *c, int kind);
 void launch_sort_due(pic_ctx *c, int mask);   // the sorts the next push of the masked species needs
 void launch_tile_push(pic_ctx *c, int mask);
+// the tile kernels' shared boxes: gather box of GE points per axis (row and
+// plane strides gsy, gsz, gsize elements), deposit box of DE (dsy, dsz, dsize)
+struct TileBoxes {
+    int GE, DE, gsy, gsz, gsize, dsy, dsz, dsize;
+};
+TileBoxes tile_boxes(const pic_ctx *c);
 size_t tile_smem_bytes(const pic_ctx *c);
 
 // adjoint_kernels.cu

@@ -668,6 +668,11 @@ static TileGeom tile_layout(const pic_ctx *c) {
     return t;
 }
 
+TileBoxes tile_boxes(const pic_ctx *c) {
+    const TileGeom t = tile_layout(c);
+    return TileBoxes{t.GE, t.DE, t.gsy, t.gsz, t.gsize, t.dsy, t.dsz, t.dsize};
+}
+
 size_t tile_smem_bytes(const pic_ctx *c) {
     const TileGeom t = tile_layout(c);
     const size_t rs = c->fp32 ? 4 : 8, nl = c->fp32 ? 2 : 3;
