@@ -433,7 +433,9 @@ __device__ __forceinline__ void box_flush(const float *scr, int lane, const Fixe
     for (int it = lane; it < nitems; it += 32) {
         const int g = it / NI, r = it - g * NI;
         const int c = r / (P + 1), pv = r - c * (P + 1);
-        const int l0 = __fns(starts, 0, g + 1);
+        unsigned rest = starts;   // drop the g lowest group starts: the next is group g's first lane
+        for (int q = 0; q < g; ++q) rest &= rest - 1u;
+        const int l0 = __ffs(rest) - 1;
         const unsigned later = l0 < 31 ? starts & (0xffffffffu << (l0 + 1)) : 0u;
         const int l1 = later ? __ffs(later) - 1 : 32;
         const int cell = __float_as_int(scr[l0 * S]);
