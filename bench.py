@@ -180,6 +180,26 @@ def count_kernel_launches(sim, steps=1):
         return None
 
 
+def measured_instructions(precision, order):
+    """Thread instructions per particle of the tiled kernel from a committed
+    ncu capture (profiles/tile_push_instructions.json: smsp__inst_executed.sum
+    x 32 / particles of one launch)."""
+    p = os.path.join(REPO, "profiles", "tile_push_instructions.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        return json.load(f)["thread_instructions_per_particle"].get(f"{precision}_o{order}")
+
+
+def issue_fraction(particles_per_s, precision, order, sm_mhz):
+    """Instruction issue rate the measured rate implies, as a fraction of the
+    issue peak (148 SMs x 4 schedulers x 32 lanes per clock)."""
+    ipp = measured_instructions(precision, order)
+    if not ipp or not sm_mhz:
+        return None
+    return particles_per_s * ipp / (148 * 4 * 32 * sm_mhz * 1e6)
+
+
 def tile_roofline(kern, npart, ncell, precision, peak, peak_kind, ms_step):
     """HBM roofline of the tiled push kernel from its CUDA-event launch
     times: algorithmic bytes per launch / average launch duration."""
@@ -229,6 +249,8 @@ def variants_bench(local, rank, warmup, steps, skip=None):
                     "cell_updates_per_s": ncell * steps / (ms / 1e3),
                     "tile_push_ms": roof["avg_launch_ms"] if roof else None,
                     "tile_push_roofline_frac": roof["frac"] if roof else None,
+                    "tile_push_issue_frac": issue_fraction(npart / (roof["avg_launch_ms"] / 1e3), prec,
+                                                           2 if mem == 2 else 4, 1965.0) if roof else None,
                     "kernels": {k: {"ms_total": v[0], "launches": v[1]} for k, v in kern.items()}})
     return out
 
@@ -628,6 +650,12 @@ def main():
     ms, npart_all, value = combine(ms, npart, args.steps, dist, device="cuda")
     peak, peak_kind = measured_peaks()
     roof = tile_roofline(kern, npart, ncell, prec, peak, peak_kind, ms)
+    if roof:
+        smhz = (clk or {}).get("sm_mhz") or 1965.0
+        roof["issue_frac"] = issue_fraction(npart / (roof["avg_launch_ms"] / 1e3), prec, w.order, smhz)
+        roof["issue_note"] = ("thread instructions per particle from an ncu capture of a smaller case of the same "
+                              "workload, times the kernel's particle rate, over 148 SMs x 4 issue slots x 32 lanes "
+                              "per clock at the sampled SM clock")
     kernels = {k: {"ms_total": v[0], "launches": v[1]} for k, v in kern.items()}
 
     extra = {}
