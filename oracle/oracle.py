@@ -124,7 +124,9 @@ class Oracle:
             for n, a in fields.items():
                 self.arrays[n][...] = a
         parts = particles if particles is not None else [np.zeros(0, PARTICLE_DTYPE)] * 2
-        self.parts = [np.ascontiguousarray(p.copy()) for p in parts]
+        # the C side reads 144-byte records: convert whatever layout came in
+        # (numpy drops the record padding when it concatenates structured arrays)
+        self.parts = [np.array(p, dtype=PARTICLE_DTYPE, copy=True, order="C") for p in parts]
         cap = max(1, max(len(p) for p in self.parts))
         self.scratch = np.zeros(cap, dtype=PARTICLE_DTYPE)
         self.g_data = None if g_data is None else np.ascontiguousarray(g_data, dtype=np.float64)

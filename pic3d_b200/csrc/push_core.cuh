@@ -259,17 +259,6 @@ struct FixedAcc {
             atomicAdd(a + lstride, (unsigned)(qi >> 20));
         }
     }
-    // A sum of up to 32 scaled contributions (|q| < 2^36), FP32: rounded
-    // to a 64-bit integer, low 20 bits and the signed rest as the two limbs
-    // (with at most kMaxTileParticles additions per point the top limb's
-    // sum stays below 2^28 in magnitude).
-    __device__ __forceinline__ void add_sum(int c, int idx, float q) const {
-        if (q == 0.0f) return;
-        unsigned *a = p[c] + idx;
-        const long long qi = __float2ll_rn(q);
-        atomicAdd(a, (unsigned)(qi & 0xFFFFF));
-        atomicAdd(a + lstride, (unsigned)(int)(qi >> 20));
-    }
 };
 
 // The middle loop of a current component over m = 0 .. len-1 (len <= P+1),
@@ -383,15 +372,6 @@ __device__ __forceinline__ void deposit(const Acc &acc, const real (&dxdt)[3], c
             }
         }
     }
-}
-
-// Where push_body hands a particle's move: the Esirkepov deposit into the
-// accumulator.  Accumulators with their own policy (the tile kernel's
-// cell-box accumulation) overload this for their type.
-template <typename real, int P, class Acc>
-__device__ __forceinline__ void deposit_particle(const Acc &acc, const real (&dxdt)[3], const Axis1D<real, P> (&ax)[3],
-                                                 bool moved, real qw) {
-    deposit<real, P>(acc, dxdt, ax, moved, qw);
 }
 
 // Decoded old position of particle p: primal / dual buffer index and
@@ -551,7 +531,7 @@ __device__ __forceinline__ void push_body(const PushArgs<real> &a, long long p, 
             moved = moved || disp[d] != real(0);
         }
     }
-    deposit_particle(acc, a.d_dt, ax, moved, qw);
+    deposit<real, P>(acc, a.d_dt, ax, moved, qw);
     // store
     a.px[p] = pxn;
     a.py[p] = pyn;

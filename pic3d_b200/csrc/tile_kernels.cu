@@ -63,11 +63,7 @@ __device__ __forceinline__ int cell_key(const TileGeom &t, int cx, int cy, int c
     const int T = t.T;
     int tx = cx / T, ty = cy / T, tz = cz / T;
     int lx = cx - tx * T, ly = cy - ty * T, lz = cz - tz * T;
-#ifdef PIC_SORT_CELL_MAJOR
-    return ((((tz * t.nt[1] + ty) * t.nt[0] + tx) * T + lz) * T * T + ly * T + lx) * kOctants + oct;
-#else
     return ((((tz * t.nt[1] + ty) * t.nt[0] + tx) * kOctants + oct) * T + lz) * T * T + ly * T + lx;
-#endif
 }
 
 // cell of a particle for sorting (FP64: periodic wrap as the next push
@@ -352,136 +348,6 @@ void launch_sort_due(pic_ctx *c, int mask) {
 }
 
 // ---------------------------------------------------------------------------
-// Cell-box current accumulation (FP32).
-//
-// A particle that stays inside the box of P + 1 points per axis around its
-// cell (b - H .. b + H + 1, b the cell's lower primal index: the supports of
-// both half-cell positions) writes its three axes' Esirkepov factors (old
-// shape s0 and difference ds over the box, zero outside its span) and its
-// component factors -q w (d/dt) scale to a per-lane slot of warp scratch
-// instead of adding into the accumulators.  After each batch of 32
-// particles the warp sums, per cell of the batch, every box point of every
-// component in registers -- one lane per (cell, component, plane), looping
-// over the cell's particles -- and adds each sum once.  J of component c at
-// box point (a_c, a_u, a_v) (a_c along c, u < v the other axes) is
-// f_c * C_c[a_c] * W(a_u, a_v), C_c the running sum of ds_c and
-// W = s0u s0v + 1/2 dsu s0v + 1/2 s0u dsv + 1/3 dsu dsv
-//   = (s0u + dsu/2)(s0v + dsv/2) + dsu dsv / 12  (src/particle.cpp:427-500).
-// Particles whose move leaves the box, and rho, go straight into the
-// accumulators.
-
-#ifndef PIC_BOX_DEPOSIT
-#define PIC_BOX_DEPOSIT 0
-#endif
-
-template <int P>
-constexpr int box_slot() { return 4 + 3 * 2 * (P + 1); }   // marker, 3 factors, 3 axes x (s0, ds)
-
-template <int P>
-struct BoxAcc {
-    FixedAcc<float, 2> fx;   // direct additions (moves leaving the box, rho)
-    float *slot;             // this lane's slot
-    int box0[3];             // buffer index of the cell box's first point per axis
-    int cell;                // the cell's index within the tile
-};
-
-template <int P>
-__device__ __forceinline__ void deposit_particle(const BoxAcc<P> &acc, const float (&dxdt)[3],
-                                                 const Axis1D<float, P> (&ax)[3], bool moved, float qw) {
-    int off[3];
-    bool fits = true;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        off[d] = ax[d].base - acc.box0[d];
-        fits = fits && off[d] >= 0 && off[d] + ax[d].len <= P + 1;
-    }
-    if (!fits) {
-        deposit<float, P>(acc.fx, dxdt, ax, moved, qw);
-        return;
-    }
-    if (acc.fx.has_rho()) deposit<float, P>(acc.fx, dxdt, ax, false, qw);   // rho only
-    if (!moved) return;
-    float *q = acc.slot;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) q[1 + c] = -qw * dxdt[c] * acc.fx.scale[c];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        float *s0 = q + 4 + d * 2 * (P + 1), *ds = s0 + (P + 1);
-#pragma unroll
-        for (int a = 0; a <= P; ++a) {
-            const int e = a - off[d];   // index into the particle's span
-            const bool in = e >= 0 && e < ax[d].len;
-            s0[a] = in ? pick(ax[d].s0, e) : 0.0f;
-            ds[a] = in ? pick(ax[d].ds, e) : 0.0f;
-        }
-    }
-    q[0] = __int_as_float(acc.cell);
-}
-
-// The batch's cells: lanes holding a slot of one cell are contiguous (the
-// particles are sorted by cell); a group starts where the marker changes.
-template <int P>
-__device__ __forceinline__ void box_flush(const float *scr, int lane, const FixedAcc<float, 2> &fx,
-                                          const int (&t0)[3], int mem, int T) {
-    constexpr int S = box_slot<P>(), H = P / 2, NI = 3 * (P + 1);
-    const int cl = __float_as_int(scr[lane * S]);
-    const int cp = __shfl_up_sync(0xffffffffu, cl, 1);
-    const unsigned starts = __ballot_sync(0xffffffffu, cl >= 0 && (lane == 0 || cp != cl));
-    const int nitems = __popc(starts) * NI;
-    const int st[3] = {1, fx.sy, fx.sz};
-#pragma unroll 1
-    for (int it = lane; it < nitems; it += 32) {
-        const int g = it / NI, r = it - g * NI;
-        const int c = r / (P + 1), pv = r - c * (P + 1);
-        unsigned rest = starts;   // drop the g lowest group starts: the next is group g's first lane
-        for (int q = 0; q < g; ++q) rest &= rest - 1u;
-        const int l0 = __ffs(rest) - 1;
-        const unsigned later = l0 < 31 ? starts & (0xffffffffu << (l0 + 1)) : 0u;
-        const int l1 = later ? __ffs(later) - 1 : 32;
-        const int cell = __float_as_int(scr[l0 * S]);
-        const int u = c == 0 ? 1 : 0, v = c == 2 ? 1 : 2;
-        float acc[P + 1][P];
-#pragma unroll
-        for (int b = 0; b <= P; ++b)
-#pragma unroll
-            for (int a = 0; a < P; ++a) acc[b][a] = 0.0f;
-#pragma unroll 1
-        for (int l = l0; l < l1; ++l) {
-            const float *q = scr + l * S;
-            if (__float_as_int(q[0]) != cell) continue;
-            const float f = q[1 + c];
-            const float *ac = q + 4 + c * 2 * (P + 1), *au = q + 4 + u * 2 * (P + 1), *av = q + 4 + v * 2 * (P + 1);
-            float C[P];
-            float run = 0.0f;
-#pragma unroll
-            for (int a = 0; a < P; ++a) {
-                run += ac[P + 1 + a];
-                C[a] = f * run;
-            }
-            const float dsv = av[P + 1 + pv];
-            const float mv = av[pv] + 0.5f * dsv, dv = dsv * (1.0f / 12.0f);
-#pragma unroll
-            for (int b = 0; b <= P; ++b) {
-                const float dsu = au[P + 1 + b];
-                const float w = (au[b] + 0.5f * dsu) * mv + dsu * dv;
-#pragma unroll
-                for (int a = 0; a < P; ++a) acc[b][a] += w * C[a];
-            }
-        }
-        // the cell's box in accumulator coordinates
-        const int lc[3] = {cell % T, (cell / T) % T, cell / (T * T)};
-        int o0 = fx.o;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) o0 += (t0[d] + lc[d] + mem - 1 - H) * st[d];
-        const int base = o0 + pv * st[v];
-#pragma unroll
-        for (int b = 0; b <= P; ++b)
-#pragma unroll
-            for (int a = 0; a < P; ++a) fx.add_sum(c, base + a * st[c] + b * st[u], acc[b][a]);
-    }
-}
-
-// ---------------------------------------------------------------------------
 // the tile kernel
 
 // limbs of the shared-memory fixed-point accumulators
@@ -575,9 +441,6 @@ __global__ void __launch_bounds__(tile_threads<real>(), tile_min_blocks<real>())
 #pragma unroll
     for (int c = 0; c < 6; ++c) fs[c] = View<const real>{sf + c * GS, gsy, gsz, -(gO[2] * gsz + gO[1] * gsy + gO[0])};
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    constexpr bool kBox = PIC_BOX_DEPOSIT && sizeof(real) == 4;
-    // cell-box scratch after the accumulators: 32 slots per warp
-    float *scr = reinterpret_cast<float *>(sa + 5 * NL * DS) + warp * 32 * box_slot<P>();
     // a warp takes 32 consecutive particles of the tile's list: mostly one
     // octant, so the lanes' primal stencils sit at the same offset from
     // their cells and their shared-memory accesses at a common stencil point
@@ -603,7 +466,6 @@ __global__ void __launch_bounds__(tile_threads<real>(), tile_min_blocks<real>())
 #pragma unroll 1
         for (long long base = (long long)warp * 32; base < m; base += (long long)nwarp * 32) {
             const long long idx = base + lane;
-            if constexpr (kBox) scr[lane * box_slot<P>()] = __int_as_float(-1);
             if (idx < m && !(a.dead && a.dead[pa[k] + idx])) {   // adjoint mode: removed particles stay, dead
                 const long long p = pa[k] + idx;
                 OldPos<real> o;
@@ -614,26 +476,11 @@ __global__ void __launch_bounds__(tile_threads<real>(), tile_min_blocks<real>())
                 if (!in_buffers(g, o, H)) {
                     set_status(a.status, ST_OOB);
                 } else if (inside) {
-                    if constexpr (kBox) {
-                        BoxAcc<P> bacc;
-                        bacc.fx = af;
-                        bacc.slot = scr + lane * box_slot<P>();
-#pragma unroll
-                        for (int d = 0; d < 3; ++d) bacc.box0[d] = o.cc[d] + g.mem - 1 - H;
-                        bacc.cell = ((o.cc[2] - t0[2]) * T + (o.cc[1] - t0[1])) * T + (o.cc[0] - t0[0]);
-                        push_body<real, P, SPIN, false>(a, p, o, fs, bacc);
-                    } else {
-                        push_body<real, P, SPIN, false>(a, p, o, fs, af);
-                    }
+                    push_body<real, P, SPIN, false>(a, p, o, fs, af);
                 } else {
                     // left its tile since the last sort: pushed by the global kernel after this one
                     ta.strag[k][atomicAdd(ta.nstrag + k, 1ull)] = (int)p;
                 }
-            }
-            if constexpr (kBox) {
-                __syncwarp();
-                box_flush<P>(scr, lane, af, t0, g.mem, T);
-                __syncwarp();
             }
         }
     }
@@ -678,10 +525,7 @@ TileBoxes tile_boxes(const pic_ctx *c) {
 size_t tile_smem_bytes(const pic_ctx *c) {
     const TileGeom t = tile_layout(c);
     const size_t rs = c->fp32 ? 4 : 8, nl = c->fp32 ? 2 : 3;
-    size_t box = 0;
-    if (PIC_BOX_DEPOSIT && c->fp32)
-        box = (size_t)(tile_threads<float>()) * (c->order == 2 ? box_slot<3>() : box_slot<5>()) * sizeof(float);
-    return 6 * (size_t)t.gsize * rs + 5 * nl * (size_t)t.dsize * 4 + box;
+    return 6 * (size_t)t.gsize * rs + 5 * nl * (size_t)t.dsize * 4;
 }
 
 template <typename real, int P, bool SPIN>

@@ -145,7 +145,10 @@ def _clustered(n_in_tile=5000, seed=3):
         extra[f] = 0.1 * rng.normal(size=n_in_tile)
     extra["gamma"] = np.sqrt(1 + extra["px"] ** 2 + extra["py"] ** 2 + extra["pz"] ** 2)
     extra["charge"], extra["mass"], extra["weight"] = -1.0, 1.0, 0.01
-    parts[0] = np.concatenate([parts[0], extra])
+    both = np.zeros(len(parts[0]) + n_in_tile, W.PARTICLE_DTYPE)   # (np.concatenate drops the record padding)
+    both[:len(parts[0])] = parts[0]
+    both[len(parts[0]):] = extra
+    parts[0] = both
     return w, parts
 
 
