@@ -379,13 +379,16 @@ struct TileArgs {
 // faster on the laser workload than 256 at 237 registers, while 384 lost
 // (a tile's 512 particles per species then leave a third of the second
 // round idle).
-template <typename real>
-constexpr int tile_min_blocks() { return sizeof(real) == 4 ? 2 : 1; }
+#ifndef PIC_FP32_O2_BLOCKS
+#define PIC_FP32_O2_BLOCKS 2
+#endif
+template <typename real, int P = 5>
+constexpr int tile_min_blocks() { return sizeof(real) == 4 ? (P == 3 ? PIC_FP32_O2_BLOCKS : 2) : 1; }
 template <typename real>
 constexpr int tile_threads() { return sizeof(real) == 4 ? 256 : 512; }
 
 template <typename real, int P, bool SPIN>
-__global__ void __launch_bounds__(tile_threads<real>(), tile_min_blocks<real>()) tile_push_kernel(TileArgs<real> ta) {
+__global__ void __launch_bounds__(tile_threads<real>(), (tile_min_blocks<real, P>())) tile_push_kernel(TileArgs<real> ta) {
     constexpr int H = P / 2;
     constexpr int NL = limbs<real>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
