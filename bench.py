@@ -55,15 +55,16 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def measured_traffic(precision):
+def measured_traffic(precision, order):
     """DRAM bytes per particle of the tiled kernel from a committed ncu
-    capture (profiles/tile_push_traffic.json); the traffic grows in
-    proportion to the particles a launch processes."""
+    capture of a smaller case of the same workload
+    (profiles/tile_push_traffic.json); the traffic grows in proportion to the
+    particles a launch processes."""
     p = os.path.join(REPO, "profiles", "tile_push_traffic.json")
     if not os.path.exists(p):
         return None
     with open(p) as f:
-        return json.load(f)["dram_bytes_per_particle"].get(precision)
+        return json.load(f)["dram_bytes_per_particle"].get(f"{precision}_o{order}")
 
 
 class Clocks:
@@ -200,7 +201,7 @@ def issue_fraction(particles_per_s, precision, order, sm_mhz):
     return particles_per_s * ipp / (148 * 4 * 32 * sm_mhz * 1e6)
 
 
-def tile_roofline(kern, npart, ncell, precision, peak, peak_kind, ms_step):
+def tile_roofline(kern, npart, ncell, precision, peak, peak_kind, ms_step, order=2):
     """HBM roofline of the tiled push kernel from its CUDA-event launch
     times: algorithmic bytes per launch / average launch duration."""
     t = kern.get("tile_push_gather_deposit")
@@ -209,7 +210,7 @@ def tile_roofline(kern, npart, ncell, precision, peak, peak_kind, ms_step):
     avg_ms = t[0] / t[1]
     per = BYTES_PER_PARTICLE[precision] + GRID_BYTES_PER_CELL[precision] * ncell / max(npart, 1)
     achieved = per * npart / (avg_ms / 1e3) / 1e9
-    tpp = measured_traffic(precision)
+    tpp = measured_traffic(precision, order)
     return {"bound": "hbm", "kernel": "tile_push_gather_deposit", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_kind": peak_kind,
             "traffic": tpp * npart if tpp else None,
@@ -243,7 +244,7 @@ def variants_bench(local, rank, warmup, steps, skip=None):
         ncell = w.nx * w.ny * w.nz
         ms, kern, _ = run_case(sim, warmup, steps)
         sim.close()
-        roof = tile_roofline(kern, npart, ncell, prec, peak, peak_kind, ms)
+        roof = tile_roofline(kern, npart, ncell, prec, peak, peak_kind, ms, 2 if mem == 2 else 4)
         out.append({"order": 2 if mem == 2 else 4, "precision": prec, "particles": npart,
                     "particle_steps_per_s": npart * steps / (ms / 1e3), "ms_per_step": ms / steps,
                     "cell_updates_per_s": ncell * steps / (ms / 1e3),
@@ -329,7 +330,7 @@ def laser_bench(local, rank, warmup_steps, steps, precision, cells=(256, 128, 12
     sim.close()
     peak, peak_kind = measured_peaks()
     ncell = w.nx * w.ny * w.nz
-    roof = tile_roofline(kern, npart, ncell, precision, peak, peak_kind, ms)
+    roof = tile_roofline(kern, npart, ncell, precision, peak, peak_kind, ms, 4)
     return {"workload": w.name, "precision": precision, "timed_after_step": warmup_steps + 1,
             "particles_at_start": npart0, "particles_timed": npart,
             "particle_steps_per_s": npart * steps / (ms / 1e3), "ms_per_step": ms / steps,
@@ -649,7 +650,7 @@ def main():
     from pic3d_b200.replicas import combine
     ms, npart_all, value = combine(ms, npart, args.steps, dist, device="cuda")
     peak, peak_kind = measured_peaks()
-    roof = tile_roofline(kern, npart, ncell, prec, peak, peak_kind, ms)
+    roof = tile_roofline(kern, npart, ncell, prec, peak, peak_kind, ms, w.order)
     if roof:
         smhz = (clk or {}).get("sm_mhz") or 1965.0
         roof["issue_frac"] = issue_fraction(npart / (roof["avg_launch_ms"] / 1e3), prec, w.order, smhz)
