@@ -75,9 +75,9 @@ typedef struct PicParams {
     int32_t adjoint;           /* 1: adjoint-capable context (stable particle order, removal marks particles dead;
                                   absorbing faces only); see pic_adjoint_* */
     int32_t absorbing;         /* extension: 1 = Silver-Mueller absorbing condition on every non-periodic face
-                                  besides x-min (y and z faces, x-max), applied after each B half-update; the
-                                  reference's x-max write (boundary.cpp:92-96) is then skipped.  0: reference
-                                  faces (y / z ghosts stay zero, conductor-like) */
+                                  besides x-min (y and z faces, x-max), applied once per step with
+                                  pic_radiating_boundary; the reference's x-max write (boundary.cpp:92-96) is
+                                  then skipped.  0: reference faces (y / z ghosts stay zero, conductor-like) */
 } PicParams;
 
 typedef struct pic_ctx pic_ctx;

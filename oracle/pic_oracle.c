@@ -198,6 +198,8 @@ static double gpulse_profile(const orc_state *s, double time, double x, double y
  * of the B ghost column at x = mem-1 (laser source at x-min) and, when the
  * x-max face is not periodic, of column local_xcells+1 (boundary.cpp:92-96;
  * for mem > 1 that column lies inside the physical region). */
+static void absorb_faces(orc_state *s);
+
 void orc_radiating_boundary(orc_state *s, int is_left, int is_right, int step) {
     geom g = make_geom(s);
     double time = step * s->dt;
@@ -240,6 +242,7 @@ void orc_radiating_boundary(orc_state *s, int is_left, int is_right, int step) {
             }
         }
     }
+    absorb_faces(s);
 }
 
 /* ------------------------------------------------------------------ */
@@ -321,13 +324,16 @@ static void update_b(orc_state *s) {
 
 /* Extension (absorbing = 1; the reference has none): the first-order
  * Silver-Mueller condition of radiating_boundary's x-min update
- * (src/boundary.cpp:88-89) on the other non-periodic faces, after every B
- * half-update.  Min faces (y, z) set the ghost B row mem-1 with the x-min
- * formula's axes relabelled cyclically; max faces (y, z, x) set the last
- * physical B row, reflected through the face (tangential B flips sign; E,
- * J and the normal B do not), from the E and J of that row and the B row
- * below it.  alpha = 1/(1 + dt/h), beta = 1 - dt/h, h the cell size across
- * the face. */
+ * (src/boundary.cpp:88-89) on the other non-periodic faces, once per step at
+ * the same point (the end of orc_radiating_boundary).  Min faces (y, z) set
+ * the ghost B row mem-1 with the x-min formula's axes relabelled cyclically;
+ * max faces (y, z, x) set the last physical B row, reflected through the
+ * face (tangential B flips sign; E and J do not), from the E and J of that
+ * row and the B row below it.  alpha = 1/(1 + dt/h), beta = 1 - dt/h, h the
+ * cell size across the face.  The x-min update's tangential-derivative term
+ * is left out: with it, relabelled onto these faces, oblique waves grow
+ * without bound (a random field in a box absorbing on every side gains 1e4
+ * per 60 steps); without it the same field decays. */
 static void absorb_faces(orc_state *s) {
     if (!s->absorbing) return;
     geom g = make_geom(s);
@@ -350,20 +356,14 @@ static void absorb_faces(orc_state *s) {
                     long c = FI(g, k, j, i), rc = RI(g, k, j, i);
                     long ct = FI(g, t[2], t[1], t[0]), cn = FI(g, n[2], n[1], n[0]);
                     if (ax == 1) {
-                        s->bx[ct] = alpha * (sg * (-2.0 * s->ez[c] - hx * (s->by[c] - s->by[FI(g, k, j, i - 1)]) -
-                                                   dt * s->jz[rc]) - beta * s->bx[cn]);
-                        s->bz[ct] = alpha * (sg * (2.0 * s->ex[c] + hz * (s->by[c] - s->by[FI(g, k - 1, j, i)]) +
-                                                   dt * s->jx[rc]) - beta * s->bz[cn]);
+                        s->bx[ct] = alpha * (sg * (-2.0 * s->ez[c] - dt * s->jz[rc]) - beta * s->bx[cn]);
+                        s->bz[ct] = alpha * (sg * (2.0 * s->ex[c] + dt * s->jx[rc]) - beta * s->bz[cn]);
                     } else if (ax == 2) {
-                        s->by[ct] = alpha * (sg * (-2.0 * s->ex[c] - hy * (s->bz[c] - s->bz[FI(g, k, j - 1, i)]) -
-                                                   dt * s->jx[rc]) - beta * s->by[cn]);
-                        s->bx[ct] = alpha * (sg * (2.0 * s->ey[c] + hx * (s->bz[c] - s->bz[FI(g, k, j, i - 1)]) +
-                                                   dt * s->jy[rc]) - beta * s->bx[cn]);
+                        s->by[ct] = alpha * (sg * (-2.0 * s->ex[c] - dt * s->jx[rc]) - beta * s->by[cn]);
+                        s->bx[ct] = alpha * (sg * (2.0 * s->ey[c] + dt * s->jy[rc]) - beta * s->bx[cn]);
                     } else {
-                        s->bz[ct] = alpha * (sg * (-2.0 * s->ey[c] - hz * (s->bx[c] - s->bx[FI(g, k - 1, j, i)]) -
-                                                   dt * s->jy[rc]) - beta * s->bz[cn]);
-                        s->by[ct] = alpha * (sg * (2.0 * s->ez[c] + hy * (s->bx[c] - s->bx[FI(g, k, j - 1, i)]) +
-                                                   dt * s->jz[rc]) - beta * s->by[cn]);
+                        s->bz[ct] = alpha * (sg * (-2.0 * s->ey[c] - dt * s->jy[rc]) - beta * s->bz[cn]);
+                        s->by[ct] = alpha * (sg * (2.0 * s->ez[c] + dt * s->jz[rc]) - beta * s->by[cn]);
                     }
                 }
     }
@@ -373,13 +373,11 @@ static void absorb_faces(orc_state *s) {
 void orc_fields_first(orc_state *s) {
     update_e(s);
     update_b(s);
-    absorb_faces(s);
 }
 
 /* update_electromagnetic_fields_second: src/field.cpp:88-117 */
 void orc_fields_second(orc_state *s) {
     update_b(s);
-    absorb_faces(s);
     update_e(s);
 }
 

@@ -15,7 +15,7 @@ void launch_update_b(pic_ctx *c, double coef);   // B -= coef curl E, then the B
 void launch_ghost_fill_one(pic_ctx *c, int array);
 void launch_fold_currents(pic_ctx *c, unsigned mask = 31u);
 void launch_radiating_boundary(pic_ctx *c, int is_left, int is_right, int step);
-void launch_absorbing_faces(pic_ctx *c);   // PicParams.absorbing extension (after each B update)
+void launch_absorbing_faces(pic_ctx *c);   // PicParams.absorbing extension (with the radiating boundary)
 void launch_binomial_pass(pic_ctx *c, int ring_index, int axis, void *scratch);
 int launch_eval(pic_ctx *c, int what, const double *in, double *d_out);
 
