@@ -379,11 +379,9 @@ struct TileArgs {
 // faster on the laser workload than 256 at 237 registers, while 384 lost
 // (a tile's 512 particles per species then leave a third of the second
 // round idle).
-#ifndef PIC_FP32_O2_BLOCKS
-#define PIC_FP32_O2_BLOCKS 2
-#endif
+// Three FP32 CTAs per SM at 2nd order measured slower than two.
 template <typename real, int P = 5>
-constexpr int tile_min_blocks() { return sizeof(real) == 4 ? (P == 3 ? PIC_FP32_O2_BLOCKS : 2) : 1; }
+constexpr int tile_min_blocks() { return sizeof(real) == 4 ? 2 : 1; }
 template <typename real>
 constexpr int tile_threads() { return sizeof(real) == 4 ? 256 : 512; }
 
@@ -399,15 +397,6 @@ __global__ void __launch_bounds__(tile_threads<real>(), (tile_min_blocks<real, P
     const int gsy = ta.t.gsy, gsz = ta.t.gsz, GS = ta.t.gsize, dsy = ta.t.dsy, dsz = ta.t.dsz, DS = ta.t.dsize;
     const int G2 = GE * GE, G3 = G2 * GE, D2 = DE * DE, D3 = D2 * DE;
     unsigned *sa = reinterpret_cast<unsigned *>(sf + 6 * GS);   // [component][limb][DS]
-#ifdef PIC_RANK_ORDER
-    // visiting order (after the 5 accumulators): per-key start and count, a
-    // few words of scan space, the list of particle offsets
-    const int T3i = ta.t.T * ta.t.T * ta.t.T * kOctants;
-    int *rk_start = reinterpret_cast<int *>(sa + 5 * NL * DS);
-    int *rk_count = rk_start + T3i;
-    int *rk_misc = rk_count + T3i;          // [0] max count, [1..32] warp totals
-    int *rk_list = rk_misc + 40;            // kMaxTileParticles entries
-#endif
     const int nacc = ta.t.nacc;
     const int tile = blockIdx.x;
     const int tx = tile % ta.t.nt[0], ty = (tile / ta.t.nt[0]) % ta.t.nt[1], tz = tile / (ta.t.nt[0] * ta.t.nt[1]);
@@ -475,67 +464,9 @@ __global__ void __launch_bounds__(tile_threads<real>(), (tile_min_blocks<real, P
         af.o = -(dO[2] * dsz + dO[1] * dsy + dO[0]);
 #pragma unroll
         for (int c = 0; c < 4; ++c) af.scale[c] = ta.scale[c];
-#ifdef PIC_RANK_ORDER
-        // Visit the tile's particles rank by rank: first the first particle
-        // of every (octant, cell) key, then the second of every key that has
-        // two, and so on.  A warp's 32 lanes then hold 32 different keys of
-        // mostly one octant, i.e. 32 different cells, so their shared loads
-        // and atomics at a common stencil offset fall in different words.
-        if (use_smem) {
-            const long long kb = (long long)tile * T3;
-            for (int key = threadIdx.x; key < T3; key += blockDim.x) {
-                long long s0 = ta.offs[k][kb + key], s1 = ta.offs[k][kb + key + 1];
-                s0 = s0 < pb[k] ? s0 : pb[k];
-                s1 = s1 < pb[k] ? s1 : pb[k];
-                rk_start[key] = (int)(s0 - pa[k]);
-                rk_count[key] = (int)(s1 > s0 ? s1 - s0 : 0);
-            }
-            if (threadIdx.x == 0) rk_misc[0] = 0;
-            __syncthreads();
-            int cmax = 0;
-            for (int key = threadIdx.x; key < T3; key += blockDim.x) cmax = max(cmax, rk_count[key]);
-            atomicMax(rk_misc, cmax);
-            __syncthreads();
-            const int maxc = rk_misc[0];
-            const int per = (T3 + (int)blockDim.x - 1) / (int)blockDim.x;   // consecutive keys per thread
-            int written = 0;
-            for (int r = 0; r < maxc; ++r) {
-                int mine = 0;
-                for (int q = 0; q < per; ++q) {
-                    const int key = threadIdx.x * per + q;
-                    mine += (key < T3 && rk_count[key] > r) ? 1 : 0;
-                }
-                int incl = mine;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int t2 = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += t2;
-                }
-                if (lane == 31) rk_misc[1 + warp] = incl;
-                __syncthreads();
-                int wbase = 0, total = 0;
-                for (int w2 = 0; w2 < nwarp; ++w2) {
-                    const int v = rk_misc[1 + w2];
-                    wbase += w2 < warp ? v : 0;
-                    total += v;
-                }
-                int pos = written + wbase + incl - mine;
-                for (int q = 0; q < per; ++q) {
-                    const int key = threadIdx.x * per + q;
-                    if (key < T3 && rk_count[key] > r) rk_list[pos++] = rk_start[key] + r;
-                }
-                written += total;
-                __syncthreads();
-            }
-        }
-#endif
 #pragma unroll 1
         for (long long base = (long long)warp * 32; base < m; base += (long long)nwarp * 32) {
-#ifdef PIC_RANK_ORDER
-            const long long idx = (use_smem && base + lane < m) ? (long long)rk_list[base + lane] : base + lane;
-#else
             const long long idx = base + lane;
-#endif
             if (idx < m && !(a.dead && a.dead[pa[k] + idx])) {   // adjoint mode: removed particles stay, dead
                 const long long p = pa[k] + idx;
                 OldPos<real> o;
@@ -553,9 +484,6 @@ __global__ void __launch_bounds__(tile_threads<real>(), (tile_min_blocks<real, P
                 }
             }
         }
-#ifdef PIC_RANK_ORDER
-        __syncthreads();   // the next species rebuilds the visiting order
-#endif
     }
     if (!use_smem) return;
     __syncthreads();
@@ -598,11 +526,7 @@ TileBoxes tile_boxes(const pic_ctx *c) {
 size_t tile_smem_bytes(const pic_ctx *c) {
     const TileGeom t = tile_layout(c);
     const size_t rs = c->fp32 ? 4 : 8, nl = c->fp32 ? 2 : 3;
-    size_t order = 0;
-#ifdef PIC_RANK_ORDER
-    order = (2 * (size_t)t.T * t.T * t.T * kOctants + 40 + kMaxTileParticles) * sizeof(int);
-#endif
-    return 6 * (size_t)t.gsize * rs + 5 * nl * (size_t)t.dsize * 4 + order;
+    return 6 * (size_t)t.gsize * rs + 5 * nl * (size_t)t.dsize * 4;
 }
 
 template <typename real, int P, bool SPIN>
