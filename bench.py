@@ -475,29 +475,49 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+FP64_SEGMENT = 50   # the FP64 record of 600 steps would not fit in HBM
+
+
+class _RoundedSpec:
+    """Mixin: initial positions and momenta rounded to FP32 (an FP64 run
+    from inputs perturbed by 1e-8 relative)."""
+
+    def base_particles(self):
+        p = super().base_particles()
+        for f in ("x", "y", "z", "px", "py", "pz"):
+            p[f] = p[f].astype("float32").astype("float64")
+        return p
+
+
 def adjoint_bench(steps=600, short_steps=100):
-    """Differentiable run: forward (with checkpoints every 50 steps) and
-    adjoint (segment recompute + reverse sweep) in FP32, the same gradient in
-    FP64, and central finite differences of the FP64 forward run at a
-    sequence of steps.
+    """Differentiable run: the FP32 forward records every push (600 steps
+    fit in HBM) and the adjoint is one reverse sweep; the same gradient in
+    FP64 (checkpoints every 50 steps, recomputed), the FP64 gradient from
+    initial conditions rounded to FP32, and central finite differences of
+    the FP64 forward run at a sequence of steps.
 
     The objective is only piecewise smooth: electrons leave through the
     absorbing faces (hundreds of thousands per 100 steps here) and each
     removal is a jump, so differences converge to the derivative only once
     the step is small enough that no removal changes step (about 1e-8 of the
-    parameter at 600 steps).  The same roughness makes the FP32 and FP64
-    derivatives differ at long horizons (the FP32 trajectory differs from the
-    FP64 one by more than that scale); the FP32 / FP64 agreement is also
-    reported at a short horizon where it is not rough."""
+    parameter at 600 steps).  At 600 steps the gradient itself is sensitive
+    at the 1e-8 level of the inputs: the FP64 gradient from FP32-rounded
+    initial conditions differs from the exact-input one by tens of percent,
+    as much as the FP32 gradient does; at 100 steps all three agree to
+    1e-6."""
     import numpy as np
 
     from pic3d_b200 import workloads as W
     from pic3d_b200.adjoint import AdjointRun, AdjointSpec, objective
 
-    def spec(prec, n=steps):
+    class RoundedSpec(_RoundedSpec, AdjointSpec):
+        pass
+
+    def spec(prec, n=steps, cls=AdjointSpec):
         w = W.differentiable_laser(precision=prec, steps=n)
-        return AdjointSpec(workload=w, n_knots=32, profile_n=8, window=(0.5 * w.nx, w.nx - 4.0), ramp=4.0,
-                           segment=50, seed=2468, precision=prec)
+        seg = n if prec == "fp32" else FP64_SEGMENT
+        return cls(workload=w, n_knots=32, profile_n=8, window=(0.5 * w.nx, w.nx - 4.0), ramp=4.0,
+                   segment=seg, seed=2468, precision=prec)
 
     rng = np.random.default_rng(13)
     knots = 0.01 + 0.02 * rng.random(32)
@@ -543,8 +563,10 @@ def adjoint_bench(steps=600, short_steps=100):
 
     rel = lambda x, y: float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
     a, b = grad(spec("fp32"), kernels=True), grad(spec("fp64"))
+    br = grad(spec("fp64", cls=RoundedSpec))
     prod32 = production_forward(spec("fp32"))
     sa, sb = grad(spec("fp32", short_steps)), grad(spec("fp64", short_steps))
+    sbr = grad(spec("fp64", short_steps, cls=RoundedSpec))
     sp64 = spec("fp64")
     checks = []
     for which, idx in [("knot", int(np.argmax(np.abs(b["gk"])))), ("laser", int(np.argmax(np.abs(b["gp"]))))]:
@@ -563,23 +585,30 @@ def adjoint_bench(steps=600, short_steps=100):
             fds[f"{rel_h:g}"] = (objective(sp64, k1, p1) - objective(sp64, k2, p2)) / (2 * h)
         checks.append({"param": f"{which}[{idx}]", "adjoint_fp64": g, "central_fd_fp64_by_relative_step": fds,
                        "rel_err_by_relative_step": {k: abs(g - f) / max(abs(f), 1e-300) for k, f in fds.items()}})
-    return {"workload": spec("fp32").workload.name, "particles": a["n"], "steps": steps, "checkpoint_every": 50,
+    return {"workload": spec("fp32").workload.name, "particles": a["n"], "steps": steps,
+            "checkpoint_every": {"fp32": steps, "fp64": FP64_SEGMENT},
             "parameters": 32 + 64, "objective": "sum s(x) w m (gamma-1), s = 1 on x in [32, 60) cells with 4-cell "
                                                   "sin^2 ramps",
             "objective_fp32": a["loss"], "objective_fp64": b["loss"],
             "forward_s": a["fwd"], "adjoint_s": a["bwd"], "adjoint_over_forward": a["bwd"] / a["fwd"],
             "production_forward_s": prod32, "adjoint_over_production_forward": a["bwd"] / prod32,
+            "forward_and_adjoint_over_production_forward": (a["fwd"] + a["bwd"]) / prod32,
             "adjoint_kernels_fp32": a["kernels"],
             "fp64_forward_s": b["fwd"], "fp64_adjoint_s": b["bwd"],
             "grad_rel_l2_fp32_vs_fp64": {"knots": rel(a["gk"], b["gk"]), "laser": rel(a["gp"], b["gp"])},
             f"grad_rel_l2_fp32_vs_fp64_{short_steps}_steps": {"knots": rel(sa["gk"], sb["gk"]),
                                                               "laser": rel(sa["gp"], sb["gp"])},
+            "grad_rel_l2_fp64_rounded_inputs_vs_fp64": {"knots": rel(br["gk"], b["gk"]),
+                                                        "laser": rel(br["gp"], b["gp"])},
+            f"grad_rel_l2_fp64_rounded_inputs_vs_fp64_{short_steps}_steps": {"knots": rel(sbr["gk"], sb["gk"]),
+                                                                             "laser": rel(sbr["gp"], sb["gp"])},
             "finite_difference_checks": checks,
-            "note": "adjoint = restore each checkpoint, recompute its 50 steps recording the push inputs, reverse "
-                    "sweep; forward = the run with checkpoints in the adjoint-capable context (tiled push, sorts "
-                    "recorded); production forward = the same run in an ordinary context; central differences of a "
+            "note": "FP32: the forward records the inputs of every push (one segment of 600 steps) and the "
+                    "adjoint is one reverse sweep; FP64: checkpoints every 50 steps, each segment recomputed while "
+                    "recording; forward = the run in the adjoint-capable context (tiled push, sorts recorded); "
+                    "production forward = the same run in an ordinary context; central differences of a "
                     "piecewise-smooth objective converge only at small steps (particle removal at the absorbing "
-                    "faces)"}
+                    "faces); rounded inputs = FP64 run from positions and momenta rounded to FP32"}
 
 
 def main():
@@ -646,6 +675,7 @@ def main():
     clocks.start()
     ms, kern = timed_steps(sim, args.steps, prof=True)
     clk = clocks.stop()
+    order_stats = [sim.particle_order_stats(k) for k in range(2)]
     sim.close()
     from pic3d_b200.replicas import combine
     ms, npart_all, value = combine(ms, npart, args.steps, dist, device="cuda")
@@ -703,12 +733,14 @@ def main():
                 "dtype": "f64" if prec == "fp64" else "f32", "data": "synthetic",
                 "config": {"workload": w.name, "cells": [w.nx, w.ny, w.nz], "order": w.order,
                            "particles": npart, "particles_per_cell": 2 * SCALEUP_PPC, "u_th": SCALEUP_UTH,
-                           "boundaries": "periodic", "tile": args.tile, "sort_interval": args.sort_interval,
+                           "boundaries": "periodic", "tile": args.tile or 4,
+                           "sort_interval": args.sort_interval or 4,
                            "parallelism": f"replicas{world}",
                            "l2": f"inputs larger than L2 (particle state {state_gb:.1f} GB)"},
                 "cell_updates_per_s": ncell * world * args.steps / (ms / 1e3),
                 "gpu_launches": int(launches_per_step * args.steps) if launches_per_step else None,
-                "roofline": roof, "kernels": kernels, "clocks": clk, "e2e": e2e, "cpu_baseline": cpu}
+                "roofline": roof, "kernels": kernels, "particle_order": order_stats, "clocks": clk, "e2e": e2e,
+                "cpu_baseline": cpu}
         line.update(extra)
         print(json.dumps(line), flush=True)
     if dist:

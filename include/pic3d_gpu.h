@@ -71,7 +71,8 @@ typedef struct PicParams {
     int32_t laser_envelope;    /* extension: 0 sine envelope (boundary.cpp:13), 1 Gaussian with intensity FWHM laser_pulse_duration */
     int32_t laser_profile;     /* extension: 0 Gaussian beam (boundary.cpp:38), 1 cubic-B-spline amplitude grid */
     int32_t tile;              /* edge of the shared-memory particle tile in cells (0: default 4, <0: no tiling) */
-    int32_t sort_interval;     /* pushes between counting sorts of the particles by cell (0: default 4) */
+    int32_t sort_interval;     /* pushes between full counting sorts of the particles by tile (0: default 4);
+                                  between sorts each push re-bins only the particles that changed tile */
     int32_t adjoint;           /* 1: adjoint-capable context (stable particle order, removal marks particles dead;
                                   absorbing faces only); see pic_adjoint_* */
     int32_t absorbing;         /* extension: 1 = Silver-Mueller absorbing condition on every non-periodic face
@@ -306,6 +307,17 @@ int pic_profile_enable(pic_ctx *ctx, int on);
 /* names[i] (static strings), total_ms[i] and launches[i] for up to cap kernels */
 int pic_profile_read(pic_ctx *ctx, const char **names, double *total_ms, int64_t *launches, int cap, int *count);
 int pic_profile_reset(pic_ctx *ctx);
+
+/* ---- particle order (tiled kernel) ------------------------------------
+ * out[0]: particles in the visitor lists the next push reads (away from
+ *         their tile's slice of the sorted arrays, pushed from the list of
+ *         the tile they are in);
+ * out[1]: 1 if those lists are complete (else the next push hands particles
+ *         away from home to the global kernel);
+ * out[2]: pushes since the last full counting sort;
+ * out[3]: particles the last push handed to the global-memory kernel.
+ * Synchronises the context's stream.                                     */
+int pic_particle_order_stats(pic_ctx *ctx, int kind, int64_t *out, int n);
 
 /* ---- checkpoint of the whole state (fields, currents, particles, step) */
 int pic_save(pic_ctx *ctx, const char *path);

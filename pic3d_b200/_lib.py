@@ -68,7 +68,7 @@ EXPORTS = [
     "pic_adjoint_backward", "pic_adjoint_weight_grad", "pic_adjoint_profile_grad", "pic_adjoint_release",
     "pic_update_fields_full", "pic_exchange_boundary", "pic_exchange_current", "pic_filter_current",
     "pic_binomial_filter_currents", "pic_deposit_particle", "pic_eval", "pic_solve_initial_field",
-    "pic_initialize_particles", "pic_generate_thermal",
+    "pic_initialize_particles", "pic_generate_thermal", "pic_particle_order_stats",
 ]
 
 # pic_eval selectors (include/pic3d_gpu.h)
@@ -132,5 +132,6 @@ def load(path: str = LIB_PATH):
     lib.pic_solve_initial_field.argtypes = [V, _D, ctypes.c_int, P(_D), ctypes.c_int]
     lib.pic_initialize_particles.argtypes = [V, ctypes.c_int, P(PicDensity), ctypes.c_int, P(_D), P(_D)]
     lib.pic_generate_thermal.argtypes = [V, ctypes.c_int, ctypes.c_int, _D, _D, ctypes.c_uint64]
+    lib.pic_particle_order_stats.argtypes = [V, ctypes.c_int, P(_I64), ctypes.c_int]
     _lib = lib
     return lib

@@ -21,15 +21,20 @@ __global__ void __launch_bounds__(256) push_kernel(PushArgs<real> a) {
     global_views(a, fv, acc);
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x) {
-        const long long p = a.idx ? (long long)a.idx[t] : t;
+        const long long p = a.idx ? (long long)a.idx[a.idx_pairs ? 2 * t : t] : t;
         if (a.dead && a.dead[p]) continue;
+        PartIn<real> in;
+        load_position(a, p, in);
         OldPos<real> o;
-        decode_old(a, p, o);
+        decode_old(a, p, in, o);
         if (!in_buffers(a.g, o, H)) {
             set_status(a.status, ST_OOB);
             continue;
         }
-        push_body<real, P, SPIN, true>(a, p, o, fv, acc);
+        int cn[3];
+        const PmSrc<real> pm{a.px, a.py, a.pz, a.w, p};
+        if (push_body<real, P, SPIN, true>(a, p, o, pm, fv, acc, cn) && a.idx_pairs)
+            vis_note(a.vsink, a.g, (int)p, a.idx[2 * t + 1], cn);
     }
 }
 
@@ -54,13 +59,16 @@ static void push_t(pic_ctx *c, int kind) {
     s.cur = 1 - s.cur;
 }
 
-// the particles listed in idx (count on the device), e.g. those the tiled
-// kernel left because they moved out of their tile since the last sort
+// the particles listed in idx as (index, home tile) pairs (count on the
+// device): those the tiled kernel left to the global kernel; each one that
+// ends away from its home tile is recorded as a visitor (when vsink is on)
 template <typename real, int P, bool SPIN>
-static void push_list_t(pic_ctx *c, int kind, const int *idx, const unsigned long long *count) {
+static void push_list_t(pic_ctx *c, int kind, const int *idx, const unsigned long long *count, const VisSink &vsink) {
     Species &s = c->sp[kind];
     PushArgs<real> a = make_push_args<real>(c, kind);
     a.idx = idx;
+    a.idx_pairs = 1;
+    a.vsink = vsink;
     a.count = reinterpret_cast<const long long *>(count);
     long long n = s.n_host;
     if (n > 0) {
@@ -70,14 +78,14 @@ static void push_list_t(pic_ctx *c, int kind, const int *idx, const unsigned lon
     }
 }
 
-void launch_push_list(pic_ctx *c, int kind, const int *idx, const unsigned long long *count) {
+void launch_push_list(pic_ctx *c, int kind, const int *idx, const unsigned long long *count, const VisSink &v) {
     bool spin = spin_active(c, kind);
     if (c->fp32) {
-        if (c->order == 2) spin ? push_list_t<float, 3, true>(c, kind, idx, count) : push_list_t<float, 3, false>(c, kind, idx, count);
-        else spin ? push_list_t<float, 5, true>(c, kind, idx, count) : push_list_t<float, 5, false>(c, kind, idx, count);
+        if (c->order == 2) spin ? push_list_t<float, 3, true>(c, kind, idx, count, v) : push_list_t<float, 3, false>(c, kind, idx, count, v);
+        else spin ? push_list_t<float, 5, true>(c, kind, idx, count, v) : push_list_t<float, 5, false>(c, kind, idx, count, v);
     } else {
-        if (c->order == 2) spin ? push_list_t<double, 3, true>(c, kind, idx, count) : push_list_t<double, 3, false>(c, kind, idx, count);
-        else spin ? push_list_t<double, 5, true>(c, kind, idx, count) : push_list_t<double, 5, false>(c, kind, idx, count);
+        if (c->order == 2) spin ? push_list_t<double, 3, true>(c, kind, idx, count, v) : push_list_t<double, 3, false>(c, kind, idx, count, v);
+        else spin ? push_list_t<double, 5, true>(c, kind, idx, count, v) : push_list_t<double, 5, false>(c, kind, idx, count, v);
     }
 }
 
@@ -160,7 +168,43 @@ struct MoveArgs {
     double *d[16];
     float *f[16];
     int *i[3];
+    // visitor lists (vsink.raw null: none): a moved particle now belongs to
+    // the sorted slice of the tile whose range holds its hole
+    VisSink vsink;
+    RemoveArgs at;          // the moved particle's position (current buffer)
+    const unsigned *offs;   // per-key start offsets of the last sort
+    long long keys_per_tile;
 };
+
+// the cell the next push's decode will see (as push_body reports it)
+__device__ __forceinline__ void current_cell(const RemoveArgs &a, long long i, int (&c)[3]) {
+    if (a.fp32) {
+        a.cp.unpack(a.cell[i], c[0], c[1], c[2]);
+        return;
+    }
+    const double v0[3] = {a.x[i], a.y[i], a.z[i]};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double v = v0[d];
+        if (a.g.per[d]) {
+            if (v < 0.0) v += a.g.n[d];
+            if (v > (double)a.g.n[d]) v -= a.g.n[d];
+        }
+        const double xc = v - (double)(1 - a.g.mem);
+        c[d] = xc >= 0.0 ? (int)xc - (a.g.mem - 1) : -1;
+    }
+}
+
+// the tile whose slice of the sorted arrays holds index i
+__device__ __forceinline__ int home_tile(const unsigned *offs, long long keys_per_tile, int ntiles, long long i) {
+    int lo = 0, hi = ntiles - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if ((long long)offs[(long long)mid * keys_per_tile] <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
 
 __global__ void apply_moves_kernel(MoveArgs a) {
     long long m = a.ctr[2];
@@ -174,11 +218,26 @@ __global__ void apply_moves_kernel(MoveArgs a) {
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) mv(a.i[k], dst, src);
+    if (a.vsink.raw) {
+        int c[3];
+        current_cell(a.at, src, c);
+        const int nt = a.vsink.nt[0] * a.vsink.nt[1] * a.vsink.nt[2];
+        vis_note(a.vsink, a.at.g, dst, home_tile(a.offs, a.keys_per_tile, nt, dst), c);
+    }
 }
 
-__global__ void finish_remove_kernel(long long *count, long long *ctr) {
-    *count = *count - ctr[0];
+// Entries the push recorded for particles that the compaction removes or
+// moves are dropped (tile -1); apply_moves records the moved ones anew.
+__global__ void vis_drop_kernel(RemoveArgs a, int *raw, const VisState *vs, long long cap) {
+    const long long n = *a.count, nn = n - a.ctr[0];
+    const long long ne = min((long long)vs->nraw, cap);
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += (long long)gridDim.x * blockDim.x) {
+        const long long i = raw[3 * e];
+        if (i >= nn || is_dead(a, i)) raw[3 * e + 2] = -1;
+    }
 }
+
+__global__ void finish_remove_kernel(long long *count, long long *ctr) { *count = *count - ctr[0]; }
 
 __global__ void mark_dead_kernel(RemoveArgs a, unsigned char *dead) {
     long long n = *a.count;
@@ -244,6 +303,13 @@ void launch_remove(pic_ctx *c, int kind) {
     m.i[1] = s.a.cell[0];
     m.i[2] = s.a.cell[1];
     (void)k;
+    if (s.vs && s.sorted) {
+        m.vsink = vis_sink_of(c, s);
+        m.at = a;
+        m.offs = s.offs;
+        m.keys_per_tile = (long long)c->tile * c->tile * c->tile * kOctants;
+        vis_drop_kernel<<<148 * 4, 256, 0, c->stream>>>(a, s.vraw, s.vs, s.vcap);
+    }
     apply_moves_kernel<<<blocks, 256, 0, c->stream>>>(m);
     finish_remove_kernel<<<1, 1, 0, c->stream>>>(s.d_count, c->d_scratch_ll);
     prof_end(c);

@@ -106,6 +106,27 @@ struct PartArrays {
 // half-cell octants per cell in the particle sort key (tile, octant, cell)
 constexpr int kOctants = 8;
 
+// Visitor-list state of one species on the device.  valid_cur: the lists
+// the running push reads name every particle that is away from its home
+// tile (else the push falls back to handing such particles to the global
+// kernel).  valid_next: the same for the entries the running push appends;
+// cleared when vraw overflows, when removal compacts the arrays, or when a
+// particle lands outside the tile grid on a periodic axis.
+struct VisState {
+    unsigned long long nraw;   // entries appended to vraw by the running push
+    unsigned valid_cur, valid_next;
+    unsigned long long nvis;   // entries of the current lists
+};
+
+// Where a push records the particles that end away from their home tile
+// (raw null: not recorded).  See Species::vraw.
+struct VisSink {
+    int *raw;                    // (index, home tile, new tile) triples
+    VisState *vs;
+    long long cap;               // triples
+    int T, nt[3];
+};
+
 struct Species {
     int64_t cap = 0;
     int64_t n_host = 0;      // host copy of the count (upper bound between syncs)
@@ -114,7 +135,20 @@ struct Species {
     PartArrays a;            // the particles
     PartArrays b;            // destination of the counting sort (same shapes)
     int *keys = nullptr;     // per-particle sort key
-    int *strag = nullptr;    // particles the tiled kernel hands to the global kernel
+    int *strag = nullptr;    // particles the tiled kernel hands to the global kernel: (index, home tile) pairs
+    // Incremental re-binning between full sorts.  A particle's home tile is
+    // the tile whose slice of the sorted arrays holds it; a particle whose
+    // cell lies in another tile is a visitor there.  Each push appends
+    // (index, home, new tile) for every particle that ends away from home
+    // (vraw); before the next push a counting sort of those entries by tile
+    // gives each tile its visitor list (vis, (index, home) pairs, vis_off).
+    int *vraw = nullptr;
+    int *vis = nullptr;
+    unsigned *vis_off = nullptr;   // ntiles + 1
+    unsigned *vis_cnt = nullptr;   // ntiles + 1 (histogram, then cursor)
+    int64_t vcap = 0;              // entries of vraw / vis
+    VisState *vs = nullptr;        // device counters and flags
+    int vis_built_for = -1;        // pushes_since_sort when the lists were last built
     unsigned char *dead = nullptr;  // adjoint mode: 1 once a particle left through an absorbing face
     // adjoint mode with tiles: the sort moves every per-particle array, so
     // the upload index travels with the particle (orig) and each sort's

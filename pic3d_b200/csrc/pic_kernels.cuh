@@ -41,7 +41,8 @@ struct ThermalArgs {
 void launch_lattice_records(pic_ctx *c, const LatticeArgs &a);
 void launch_thermal_records(pic_ctx *c, const ThermalArgs &a);
 void launch_push(pic_ctx *c, int kind);
-void launch_push_list(pic_ctx *c, int kind, const int *idx, const unsigned long long *count);
+// idx: (index, home tile) pairs; visitors recorded into v when v.raw is set
+void launch_push_list(pic_ctx *c, int kind, const int *idx, const unsigned long long *count, const VisSink &v);
 void launch_remove(pic_ctx *c, int kind);
 void launch_upload_particles(pic_ctx *c, int kind, const void *d_records, int64_t n, int64_t offset,
                              unsigned long long *check = nullptr);
@@ -54,6 +55,8 @@ void launch_deposit_one(pic_ctx *c, int kind, const double (&xo)[3], const doubl
 void launch_sort(pic_ctx *c, int kind);
 void launch_sort_due(pic_ctx *c, int mask);   // the sorts the next push of the masked species needs
 void launch_tile_push(pic_ctx *c, int mask);
+int tile_order_stats(pic_ctx *c, int kind, long long (&out)[4]);
+VisSink vis_sink_of(const pic_ctx *c, const Species &s);   // where a push of species s records visitors
 // the tile kernels' shared boxes: gather box of GE points per axis (row and
 // plane strides gsy, gsz, gsize elements), deposit box of DE (dsy, dsz, dsize)
 struct TileBoxes {

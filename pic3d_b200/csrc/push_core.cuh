@@ -11,6 +11,49 @@
 
 namespace pic {
 
+// Record particle p (home tile `home`) if its new cell lies in another tile.
+// A cell outside the grid on a periodic axis (an FP64 position exactly at
+// x = n, wrapped only at the next push) cannot be binned: the next push
+// falls back to the global kernel for particles away from home.  Outside on
+// a non-periodic axis the particle is removed before the next push.
+// `here`, `lo`: a tile the cell is likely in (the pushing CTA's) and its
+// first cell per axis (here < 0: none), which spares the divisions.
+__device__ __forceinline__ void vis_note(const VisSink &v, const Geom &g, int p, int home, const int (&cell)[3],
+                                         int here = -1, const int *lo = nullptr) {
+    if (!v.raw) return;
+    int t = -1;
+    if (here >= 0) {
+        bool in_here = true;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) in_here = in_here && cell[d] >= lo[d] && cell[d] < lo[d] + v.T;
+        if (in_here) t = here;
+    }
+    if (t == home) return;
+    if (t < 0) {
+        bool in = true, per_out = false;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const bool o = cell[d] < 0 || cell[d] >= g.n[d];
+            in = in && !o;
+            per_out = per_out || (o && g.per[d]);
+        }
+        if (!in) {
+            if (per_out) v.vs->valid_next = 0u;
+            return;
+        }
+        t = ((cell[2] / v.T) * v.nt[1] + cell[1] / v.T) * v.nt[0] + cell[0] / v.T;
+        if (t == home) return;
+    }
+    const unsigned long long s = atomicAdd(&v.vs->nraw, 1ull);
+    if ((long long)s >= v.cap) {
+        v.vs->valid_next = 0u;
+        return;
+    }
+    v.raw[3 * s] = p;
+    v.raw[3 * s + 1] = home;
+    v.raw[3 * s + 2] = t;
+}
+
 template <typename real>
 struct PushArgs {
     Geom g;
@@ -18,6 +61,8 @@ struct PushArgs {
     real *jx, *jy, *jz, *rho;
     const long long *count;
     const int *idx;          // optional list of particle indices (count entries); null: all particles
+    int idx_pairs;           // idx holds (index, home tile) pairs
+    VisSink vsink;           // visitor recording (raw null: off)
     const unsigned char *dead;   // adjoint mode: particles already removed are skipped (null otherwise)
     // FP64 positions (cur -> nxt)
     double *x0, *y0, *z0;
@@ -386,14 +431,59 @@ struct OldPos {
     real oo[3];
 };
 
+// What one push reads of particle p: FP64 position (x, y, z) or FP32 packed
+// cell + offsets, then momenta and weight, as words of the precision's size
+// (so that the tile kernel can stage them with asynchronous copies).
 template <typename real>
-__device__ __forceinline__ void decode_old(const PushArgs<real> &a, long long p, OldPos<real> &o) {
+struct PartIn {
+    using word = typename cuda::std::conditional<sizeof(real) == 8, unsigned long long, unsigned>::type;
+    static constexpr int kWords = sizeof(real) == 8 ? 7 : 8;   // all inputs
+    static constexpr int kPos = sizeof(real) == 8 ? 3 : 4;     // the position words
+    word v[kWords];
+};
+
+// where push_body reads momenta and weight: the particle arrays (i = the
+// particle) or rows of the tile kernel's staging buffer (i = the lane)
+template <typename real>
+struct PmSrc {
+    const real *px, *py, *pz, *w;
+    long long i;
+};
+
+template <typename real>
+__device__ __forceinline__ const typename PartIn<real>::word *particle_word_src(const PushArgs<real> &a, long long p,
+                                                                                 int k) {
+    using word = typename PartIn<real>::word;
+    if constexpr (sizeof(real) == 8) {
+        const double *src[7] = {a.x0, a.y0, a.z0, a.px, a.py, a.pz, a.w};
+        return reinterpret_cast<const word *>(src[k] + p);
+    } else {
+        const void *src[8] = {a.c0, a.ox0, a.oy0, a.oz0, a.px, a.py, a.pz, a.w};
+        return reinterpret_cast<const word *>(src[k]) + p;
+    }
+}
+
+template <typename real>
+__device__ __forceinline__ void load_position(const PushArgs<real> &a, long long p, PartIn<real> &in) {
+#pragma unroll
+    for (int k = 0; k < PartIn<real>::kPos; ++k) in.v[k] = *particle_word_src(a, p, k);
+}
+
+template <typename real>
+__device__ __forceinline__ real part_real(const PartIn<real> &in, int k) {
+    if constexpr (sizeof(real) == 8) return __longlong_as_double((long long)in.v[k]);
+    else return __uint_as_float(in.v[k]);
+}
+
+template <typename real>
+__device__ __forceinline__ void decode_old(const PushArgs<real> &a, long long p, const PartIn<real> &in,
+                                           OldPos<real> &o) {
     constexpr bool F64 = cuda::std::is_same<real, double>::value;
     const Geom &g = a.g;
     if constexpr (F64) {
-        o.xd[0] = a.x0[p];
-        o.xd[1] = a.y0[p];
-        o.xd[2] = a.z0[p];
+        o.xd[0] = part_real(in, 0);
+        o.xd[1] = part_real(in, 1);
+        o.xd[2] = part_real(in, 2);
         bool wrapped = false;
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
@@ -416,10 +506,10 @@ __device__ __forceinline__ void decode_old(const PushArgs<real> &a, long long p,
             o.dd[d] = (xc - 0.5) - (double)o.id[d];
         }
     } else {
-        a.cp.unpack(a.c0[p], o.cc[0], o.cc[1], o.cc[2]);
-        o.oo[0] = a.ox0[p];
-        o.oo[1] = a.oy0[p];
-        o.oo[2] = a.oz0[p];
+        a.cp.unpack((int)in.v[0], o.cc[0], o.cc[1], o.cc[2]);
+        o.oo[0] = __uint_as_float(in.v[1]);
+        o.oo[1] = __uint_as_float(in.v[2]);
+        o.oo[2] = __uint_as_float(in.v[3]);
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             int b = o.cc[d] + g.mem - 1;
@@ -435,9 +525,13 @@ __device__ __forceinline__ void decode_old(const PushArgs<real> &a, long long p,
 // Everything after the position decode: gather, Boris, move, deposit,
 // store, spin.  fv: the six field views; jv: view for the current arrays
 // (jx..rho share its strides).
+// Returns false when the particle was skipped (non-finite momentum or a move
+// over a cell: status set, nothing stored); else cnew is its new cell as the
+// next push's decode will see it.
 template <typename real, int P, bool SPIN, bool LDG, class Acc>
-__device__ __forceinline__ void push_body(const PushArgs<real> &a, long long p, const OldPos<real> &o,
-                                          const View<const real> (&fv)[6], const Acc &acc) {
+__device__ __forceinline__ bool push_body(const PushArgs<real> &a, long long p, const OldPos<real> &o,
+                                          const PmSrc<real> &pm, const View<const real> (&fv)[6], const Acc &acc,
+                                          int (&cnew)[3]) {
     constexpr bool F64 = cuda::std::is_same<real, double>::value;
     constexpr int H = P / 2;
     const Geom &g = a.g;
@@ -459,7 +553,7 @@ __device__ __forceinline__ void push_body(const PushArgs<real> &a, long long p, 
     const real qm = a.qm;
     real ex_p = e0 * qm, ey_p = e1 * qm, ez_p = e2 * qm;
     real bx_p = b0 * qm, by_p = b1 * qm, bz_p = b2 * qm;
-    real px1 = a.px[p] + ex_p, py1 = a.py[p] + ey_p, pz1 = a.pz[p] + ez_p;
+    real px1 = pm.px[pm.i] + ex_p, py1 = pm.py[pm.i] + ey_p, pz1 = pm.pz[pm.i] + ez_p;
     real gm1 = sqrt(real(1) + (px1 * px1 + py1 * py1 + pz1 * pz1));
     real tx = bx_p / gm1, ty = by_p / gm1, tz = bz_p / gm1;
     real tt = real(2) / (real(1) + tx * tx + ty * ty + tz * tz);
@@ -513,9 +607,9 @@ __device__ __forceinline__ void push_body(const PushArgs<real> &a, long long p, 
     bool cfl = abs(i2[0] - ip[0]) <= 1 && abs(i2[1] - ip[1]) <= 1 && abs(i2[2] - ip[2]) <= 1;
     if (!fin || !cfl) {
         set_status(a.status, fin ? ST_CFL : ST_NAN);
-        return;
+        return false;
     }
-    const real qw = a.charge * a.w[p];
+    const real qw = a.charge * pm.w[pm.i];
     Axis1D<real, P> ax[3];
     bool moved = false;
     if constexpr (F64) {
@@ -540,10 +634,23 @@ __device__ __forceinline__ void push_body(const PushArgs<real> &a, long long p, 
         a.x1[p] = xn[0];
         a.y1[p] = xn[1];
         a.z1[p] = xn[2];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            // the wrap and truncation of decode_old
+            double v = xn[d];
+            if (g.per[d]) {
+                if (v < 0.0) v += g.n[d];
+                if (v > (double)g.n[d]) v -= g.n[d];
+            }
+            const double xc = v - (double)(1 - g.mem);
+            cnew[d] = xc >= 0.0 ? (int)xc - (g.mem - 1) : -1;
+        }
     } else {
 #pragma unroll
-        for (int d = 0; d < 3; ++d)
+        for (int d = 0; d < 3; ++d) {
             if (g.per[d]) cn[d] = cn[d] < 0 ? cn[d] + g.n[d] : (cn[d] >= g.n[d] ? cn[d] - g.n[d] : cn[d]);
+            cnew[d] = cn[d];
+        }
         a.c1[p] = a.cp.pack(cn[0], cn[1], cn[2]);
         a.ox1[p] = on[0];
         a.oy1[p] = on[1];
@@ -582,6 +689,7 @@ __device__ __forceinline__ void push_body(const PushArgs<real> &a, long long p, 
             a.sz[p] = (real)(s_z + (rx * uy - ry * ux) * t2);
         }
     }
+    return true;
 }
 
 // bounds check of the old position against the global buffers: the whole

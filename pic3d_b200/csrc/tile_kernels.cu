@@ -259,6 +259,58 @@ __global__ void scatter_kernel(ScatterArgs a) {
     if (a.perm) a.perm[dst] = (int)i;
 }
 
+// ---------------------------------------------------------------------------
+// visitor lists: a counting sort by tile of the (index, home, tile) entries
+// the last push recorded
+
+__global__ void vis_reset_kernel(VisState *vs) {
+    vs->nraw = 0;
+    vs->nvis = 0;
+    vs->valid_cur = 1u;
+    vs->valid_next = 1u;
+}
+
+// entries with tile -1 were dropped by the removal compaction
+__global__ void vis_hist_kernel(const int *raw, const VisState *vs, long long cap, unsigned *cnt) {
+    const long long n = min((long long)vs->nraw, cap);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        if (raw[3 * i + 2] >= 0) atomicAdd(&cnt[raw[3 * i + 2]], 1u);
+}
+
+__global__ void vis_scatter_kernel(const int *raw, const VisState *vs, long long cap, unsigned *cursor, int *vis) {
+    const long long n = min((long long)vs->nraw, cap);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        if (raw[3 * i + 2] < 0) continue;
+        const unsigned slot = atomicAdd(&cursor[raw[3 * i + 2]], 1u);
+        vis[2 * slot] = raw[3 * i];
+        vis[2 * slot + 1] = raw[3 * i + 1];
+    }
+}
+
+// the lists just built are the ones the coming push reads; it records into
+// an empty raw list
+__global__ void vis_rotate_kernel(VisState *vs, long long cap) {
+    vs->nvis = min((long long)vs->nraw, cap);
+    vs->valid_cur = vs->valid_next;
+    vs->nraw = 0;
+    vs->valid_next = 1u;
+}
+
+static void launch_vis_build(pic_ctx *c, Species &s) {
+    const long long nt = (long long)c->ntile[0] * c->ntile[1] * c->ntile[2];
+    const int per_block = 1024 * 4;
+    const int sb = (int)((nt + per_block - 1) / per_block);
+    const unsigned grid = 148 * 4;
+    cudaMemsetAsync(s.vis_cnt, 0, (size_t)(nt + 1) * sizeof(unsigned), c->stream);
+    vis_hist_kernel<<<grid, 256, 0, c->stream>>>(s.vraw, s.vs, s.vcap, s.vis_cnt);
+    scan_blocks_kernel<<<sb, 1024, 0, c->stream>>>(s.vis_cnt, nt, c->d_blocksums);
+    scan_sums_kernel<<<1, 1024, 0, c->stream>>>(c->d_blocksums, sb);
+    scan_add_kernel<<<(unsigned)((nt + 1 + 255) / 256), 256, 0, c->stream>>>(s.vis_cnt, nt, c->d_blocksums, per_block,
+                                                                             s.vis_off, s.vis_cnt);
+    vis_scatter_kernel<<<grid, 256, 0, c->stream>>>(s.vraw, s.vs, s.vcap, s.vis_cnt, s.vis);
+    vis_rotate_kernel<<<1, 1, 0, c->stream>>>(s.vs, s.vcap);
+}
+
 static TileGeom tile_geom(const pic_ctx *c) {
     TileGeom t{};
     t.T = c->tile;
@@ -300,7 +352,10 @@ void launch_sort(pic_ctx *c, int kind) {
     sa.status = c->d_status;
     sa.keys = s.keys;
     sa.cursor = c->d_hist;
+    // The sort runs right before a push, which overwrites the previous-position
+    // buffer: only the current one moves (the adjoint's tape keeps both).
     for (int b = 0; b < 2; ++b) {
+        if (b != s.cur && !c->p.adjoint) continue;
         if (c->fp32) {
             sa.fs[sa.nf] = s.a.ox[b]; sa.fd[sa.nf++] = s.b.ox[b];
             sa.fs[sa.nf] = s.a.oy[b]; sa.fd[sa.nf++] = s.b.oy[b];
@@ -335,6 +390,12 @@ void launch_sort(pic_ctx *c, int kind) {
     }
     s.sorted = true;
     s.pushes_since_sort = 0;
+    if (s.vs) {   // every particle is at home: empty visitor lists
+        cudaMemsetAsync(s.vis_off, 0, (size_t)(c->ntile[0] * c->ntile[1] * c->ntile[2] + 1) * sizeof(unsigned),
+                        c->stream);
+        vis_reset_kernel<<<1, 1, 0, c->stream>>>(s.vs);
+    }
+    s.vis_built_for = 0;
     prof_end(c);
 }
 
@@ -344,6 +405,24 @@ void launch_sort_due(pic_ctx *c, int mask) {
         Species &s = c->sp[k];
         if (!((mask >> k) & 1) || s.n_host <= 0) continue;
         if (!s.sorted || s.pushes_since_sort >= c->sort_interval) launch_sort(c, k);
+    }
+}
+
+// Before a push: a full sort when due, else this push's visitor lists from
+// what the last push recorded (once per push: pushes_since_sort counts them).
+static void prepare_push(pic_ctx *c, int mask) {
+    if (c->tile <= 0) return;
+    for (int k = 0; k < 2; ++k) {
+        Species &s = c->sp[k];
+        if (!((mask >> k) & 1) || s.n_host <= 0) continue;
+        if (!s.sorted || s.pushes_since_sort >= c->sort_interval) {
+            launch_sort(c, k);
+        } else if (s.vs && s.vis_built_for != s.pushes_since_sort) {
+            prof_begin(c, "visitor_lists");
+            launch_vis_build(c, s);
+            prof_end(c);
+        }
+        s.vis_built_for = s.pushes_since_sort;
     }
 }
 
@@ -358,6 +437,22 @@ constexpr int limbs() { return sizeof(real) == 8 ? 3 : 2; }
 // reassembled total in 64 bits
 constexpr int kMaxTileParticles = 4095;
 
+// Asynchronous global -> shared copies (cp.async): a CTA issues every copy
+// of a batch without waiting on any, then waits once.  src_bytes 0 fills the
+// destination with zeros and reads nothing.
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *dst, const void *src, int src_bytes = BYTES) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(src), "n"(BYTES), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// word offset (from the accumulators) of the particle input buffers: after
+// the five accumulators, rounded up to 16 bytes
+__host__ __device__ constexpr int particle_buffer_offset(int acc_words) { return (acc_words + 3) & ~3; }
+
 template <typename real>
 struct TileArgs {
     PushArgs<real> sp[2];
@@ -368,8 +463,14 @@ struct TileArgs {
     const real *field[6];
     real scale[4];          // jx, jy, jz, rho
     double inv_scale[4];
-    int *strag[2];          // indices of particles left for the global kernel
+    int *strag[2];          // (index, home tile) of particles left for the global kernel
     unsigned long long *nstrag;
+    // visitor lists of this push (vis_off null: none) and the recording of
+    // the next push's (vsink.raw null: off)
+    const int *vis[2];
+    const unsigned *vis_off[2];
+    const VisState *vs[2];
+    VisSink vsink[2];
 };
 
 // Threads per CTA and CTAs per SM the register allocation must allow.
@@ -397,6 +498,13 @@ __global__ void __launch_bounds__(tile_threads<real>(), (tile_min_blocks<real, P
     const int gsy = ta.t.gsy, gsz = ta.t.gsz, GS = ta.t.gsize, dsy = ta.t.dsy, dsz = ta.t.dsz, DS = ta.t.dsize;
     const int G2 = GE * GE, G3 = G2 * GE, D2 = DE * DE, D3 = D2 * DE;
     unsigned *sa = reinterpret_cast<unsigned *>(sf + 6 * GS);   // [component][limb][DS]
+    // per warp, two slots of one batch of particle inputs, [word][lane],
+    // and the (index, home tile) of each lane's particle per slot
+    using PWord = typename PartIn<real>::word;
+    constexpr int KW = PartIn<real>::kWords;
+    PWord *sp_in = reinterpret_cast<PWord *>(sa + particle_buffer_offset(5 * NL * DS)) + (threadIdx.x >> 5) * 2 * KW * 32;
+    int2 *sp_loc = reinterpret_cast<int2 *>(reinterpret_cast<PWord *>(sa + particle_buffer_offset(5 * NL * DS)) +
+                                            (blockDim.x >> 5) * 2 * KW * 32) + (threadIdx.x >> 5) * 2 * 32;
     const int nacc = ta.t.nacc;
     const int tile = blockIdx.x;
     const int tx = tile % ta.t.nt[0], ty = (tile / ta.t.nt[0]) % ta.t.nt[1], tz = tile / (ta.t.nt[0] * ta.t.nt[1]);
@@ -407,9 +515,11 @@ __global__ void __launch_bounds__(tile_threads<real>(), (tile_min_blocks<real, P
         gO[d] = t0[d] + g.mem - 1 - H;   // field buffer coordinate of the first staged point
         dO[d] = t0[d] + g.mem - 2 - H;   // buffer coordinate of the first accumulator point
     }
-    // particle ranges of this tile
+    // particle ranges of this tile: its slice of the sorted arrays (home
+    // particles) and its visitor list
     const long long T3 = (long long)T * T * T * kOctants;   // keys per tile
-    long long pa[2] = {0, 0}, pb[2] = {0, 0};
+    long long pa[2] = {0, 0}, pb[2] = {0, 0}, va[2] = {0, 0}, vb[2] = {0, 0};
+    bool vvalid[2] = {false, false};
     long long mtot = 0;
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
@@ -419,23 +529,30 @@ __global__ void __launch_bounds__(tile_threads<real>(), (tile_min_blocks<real, P
         pb[k] = ta.offs[k][(tile + 1) * T3];
         pb[k] = pb[k] < n ? pb[k] : n;
         if (pa[k] > pb[k]) pa[k] = pb[k];
-        mtot += pb[k] - pa[k];
+        vvalid[k] = ta.vs[k] && ta.vs[k]->valid_cur;
+        if (vvalid[k] && ta.vis_off[k]) {
+            va[k] = ta.vis_off[k][tile];
+            vb[k] = ta.vis_off[k][tile + 1];
+        }
+        mtot += pb[k] - pa[k] + vb[k] - va[k];
     }
     if (mtot == 0) return;
     const bool use_smem = mtot <= kMaxTileParticles;
-    // 1. stage fields, 2. clear accumulators
+    // 1. stage fields (asynchronous copies; points outside the buffers read
+    // as zero), 2. clear accumulators
     if (use_smem) {
         for (int e = threadIdx.x; e < 6 * G3; e += blockDim.x) {
             int c = e / G3, l = e - c * G3;
             int lz = l / G2, r = l - lz * G2, ly = r / GE, lx = r - ly * GE;
             int x = gO[0] + lx, y = gO[1] + ly, z = gO[2] + lz;
-            real v = 0;
-            if (x >= 0 && x < g.f[0] && y >= 0 && y < g.f[1] && z >= 0 && z < g.f[2])
-                v = __ldg(ta.field[c] + g.fi(z, y, x));
-            sf[c * GS + lz * gsz + ly * gsy + lx] = v;
+            const bool in = x >= 0 && x < g.f[0] && y >= 0 && y < g.f[1] && z >= 0 && z < g.f[2];
+            cp_async<sizeof(real)>(sf + c * GS + lz * gsz + ly * gsy + lx,
+                                   ta.field[c] + (in ? g.fi(z, y, x) : 0), in ? (int)sizeof(real) : 0);
         }
+        cp_async_commit();
         for (int e = threadIdx.x; e < nacc * NL * DS; e += blockDim.x) sa[e] = 0u;
     }
+    cp_async_wait_all();
     __syncthreads();
 
     View<const real> fs[6];
@@ -451,9 +568,10 @@ __global__ void __launch_bounds__(tile_threads<real>(), (tile_min_blocks<real, P
     // 3. particles of both species
 #pragma unroll 1
     for (int k = 0; k < 2; ++k) {
-        if (pb[k] <= pa[k]) continue;
+        const long long mh = pb[k] - pa[k];         // home particles, then visitors
+        const long long m = mh + vb[k] - va[k];
+        if (m <= 0) continue;
         const PushArgs<real> &a = ta.sp[k];
-        const long long m = pb[k] - pa[k];
         FixedAcc<real, NL> af;
 #pragma unroll
         for (int c = 0; c < 3; ++c) af.p[c] = sa + c * NL * DS;
@@ -464,26 +582,67 @@ __global__ void __launch_bounds__(tile_threads<real>(), (tile_min_blocks<real, P
         af.o = -(dO[2] * dsz + dO[1] * dsy + dO[0]);
 #pragma unroll
         for (int c = 0; c < 4; ++c) af.scale[c] = ta.scale[c];
+        // The particle of list position i: a home particle, or an entry of
+        // the visitor list.  Its inputs are copied asynchronously into slot
+        // `slot` of this warp's buffer one batch ahead of its push.
+        const long long pak = pa[k];
+        const int2 *visk = reinterpret_cast<const int2 *>(ta.vis[k]) + va[k];
+        auto prefetch = [&](long long i, int slot) {
+            if (i >= m) return;
+            int2 e = make_int2((int)(pak + i), tile);
+            if (i >= mh) e = visk[i - mh];
+            sp_loc[slot * 32 + lane] = e;
+            PWord *dst = sp_in + slot * KW * 32 + lane;
+#pragma unroll
+            for (int w = 0; w < KW; ++w) cp_async<sizeof(PWord)>(dst + w * 32, particle_word_src(a, (long long)e.x, w));
+        };
+        long long idx = (long long)warp * 32 + lane;
+        int slot = 0;
+        prefetch(idx, 0);
+        cp_async_commit();
 #pragma unroll 1
         for (long long base = (long long)warp * 32; base < m; base += (long long)nwarp * 32) {
-            const long long idx = base + lane;
-            if (idx < m && !(a.dead && a.dead[pa[k] + idx])) {   // adjoint mode: removed particles stay, dead
-                const long long p = pa[k] + idx;
+            cp_async_wait_all();
+            const int2 loc = sp_loc[slot * 32 + lane];
+            const long long p = loc.x;
+            const int home = loc.y;
+            const bool dead = idx < m && a.dead && a.dead[p];   // adjoint mode: removed particles stay, dead
+            // the next batch into the other slot
+            prefetch(idx + (long long)nwarp * 32, slot ^ 1);
+            cp_async_commit();
+            const PWord *row = sp_in + slot * KW * 32 + lane;
+            if (idx < m && !dead) {
+                PartIn<real> in;
+#pragma unroll
+                for (int w = 0; w < PartIn<real>::kPos; ++w) in.v[w] = row[w * 32];
                 OldPos<real> o;
-                decode_old(a, p, o);
-                bool inside = use_smem;
+                decode_old(a, p, in, o);
+                bool inside = true;
 #pragma unroll
                 for (int d = 0; d < 3; ++d) inside = inside && o.id[d] >= lo_id[d] && o.id[d] < lo_id[d] + T;
                 if (!in_buffers(g, o, H)) {
                     set_status(a.status, ST_OOB);
-                } else if (inside) {
-                    push_body<real, P, SPIN, false>(a, p, o, fs, af);
+                } else if (inside && use_smem) {
+                    int cn[3];
+                    constexpr int mo = PartIn<real>::kPos;   // momenta, then weight
+                    const real *pr = reinterpret_cast<const real *>(sp_in + slot * KW * 32);
+                    const PmSrc<real> pm{pr + mo * 32, pr + (mo + 1) * 32, pr + (mo + 2) * 32, pr + (mo + 3) * 32, lane};
+                    if (push_body<real, P, SPIN, false>(a, p, o, pm, fs, af, cn))
+                        vis_note(ta.vsink[k], g, (int)p, home, cn, tile, t0);
+                } else if (!inside && idx < mh && vvalid[k]) {
+                    // away from home: pushed from the visitor list of the tile it is in
                 } else {
-                    // left its tile since the last sort: pushed by the global kernel after this one
-                    ta.strag[k][atomicAdd(ta.nstrag + k, 1ull)] = (int)p;
+                    // a crowded tile, or away from home without valid visitor
+                    // lists: pushed by the global kernel after this one
+                    const unsigned long long q = atomicAdd(ta.nstrag + k, 1ull);
+                    ta.strag[k][2 * q] = (int)p;
+                    ta.strag[k][2 * q + 1] = home;
                 }
             }
+            idx += (long long)nwarp * 32;
+            slot ^= 1;
         }
+        cp_async_wait_all();
     }
     if (!use_smem) return;
     __syncthreads();
@@ -526,7 +685,21 @@ TileBoxes tile_boxes(const pic_ctx *c) {
 size_t tile_smem_bytes(const pic_ctx *c) {
     const TileGeom t = tile_layout(c);
     const size_t rs = c->fp32 ? 4 : 8, nl = c->fp32 ? 2 : 3;
-    return 6 * (size_t)t.gsize * rs + 5 * nl * (size_t)t.dsize * 4;
+    const size_t warps = (c->fp32 ? tile_threads<float>() : tile_threads<double>()) / 32;
+    const size_t words = c->fp32 ? PartIn<float>::kWords : PartIn<double>::kWords;
+    return 6 * (size_t)t.gsize * rs + 4 * (size_t)particle_buffer_offset((int)(5 * nl * t.dsize)) +
+           warps * 2 * 32 * (words * rs + sizeof(int2));
+}
+
+VisSink vis_sink_of(const pic_ctx *c, const Species &s) {
+    VisSink v{};
+    if (!s.vs) return v;
+    v.raw = s.vraw;
+    v.vs = s.vs;
+    v.cap = s.vcap;
+    v.T = c->tile;
+    for (int d = 0; d < 3; ++d) v.nt[d] = c->ntile[d];
+    return v;
 }
 
 template <typename real, int P, bool SPIN>
@@ -555,7 +728,14 @@ static void tile_push_t(pic_ctx *c, int mask) {
         ta.scale[k] = (real)s;
         ta.inv_scale[k] = 1.0 / (double)ta.scale[k];
     }
-    for (int k = 0; k < 2; ++k) ta.strag[k] = c->sp[k].strag;
+    for (int k = 0; k < 2; ++k) {
+        Species &s = c->sp[k];
+        ta.strag[k] = s.strag;
+        ta.vis[k] = s.vis;
+        ta.vis_off[k] = s.vis_off;
+        ta.vs[k] = s.vs;
+        ta.vsink[k] = vis_sink_of(c, s);
+    }
     ta.nstrag = c->d_nstrag;
     cudaMemsetAsync(c->d_nstrag, 0, 2 * sizeof(unsigned long long), c->stream);
     size_t smem = tile_smem_bytes(c);
@@ -564,8 +744,31 @@ static void tile_push_t(pic_ctx *c, int mask) {
     tile_push_kernel<real, P, SPIN><<<ntiles, tile_threads<real>(), smem, c->stream>>>(ta);
 }
 
+// the counts pic_particle_order_stats reports (host side, synchronising)
+int tile_order_stats(pic_ctx *c, int kind, long long (&out)[4]) {
+    Species &s = c->sp[kind];
+    out[0] = out[1] = out[3] = 0;
+    out[2] = s.pushes_since_sort;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return PIC_ECUDA;
+    if (s.vs && s.sorted) {
+        // the lists the next push will read: built from what the last push
+        // recorded unless a full sort comes first
+        VisState v{};
+        if (cudaMemcpy(&v, s.vs, sizeof v, cudaMemcpyDeviceToHost) != cudaSuccess) return PIC_ECUDA;
+        const bool built = s.vis_built_for == s.pushes_since_sort;
+        out[0] = built ? (long long)v.nvis : std::min<long long>((long long)v.nraw, s.vcap);
+        out[1] = built ? v.valid_cur : v.valid_next;
+    }
+    if (c->d_nstrag) {
+        unsigned long long ns[2] = {0, 0};
+        if (cudaMemcpy(ns, c->d_nstrag, sizeof ns, cudaMemcpyDeviceToHost) != cudaSuccess) return PIC_ECUDA;
+        out[3] = (long long)ns[kind];
+    }
+    return PIC_OK;
+}
+
 void launch_tile_push(pic_ctx *c, int mask) {
-    launch_sort_due(c, mask);
+    prepare_push(c, mask);
     bool spin = ((mask & 1) && spin_active(c, 0)) || ((mask & 2) && spin_active(c, 1));
     prof_begin(c, "tile_push_gather_deposit");
     if (c->fp32) {
@@ -578,7 +781,8 @@ void launch_tile_push(pic_ctx *c, int mask) {
     prof_end(c);
     prof_begin(c, "straggler_push");
     for (int k = 0; k < 2; ++k)
-        if (((mask >> k) & 1) && c->sp[k].n_host > 0) launch_push_list(c, k, c->sp[k].strag, c->d_nstrag + k);
+        if (((mask >> k) & 1) && c->sp[k].n_host > 0)
+            launch_push_list(c, k, c->sp[k].strag, c->d_nstrag + k, vis_sink_of(c, c->sp[k]));
     prof_end(c);
     for (int k = 0; k < 2; ++k) {
         Species &s = c->sp[k];

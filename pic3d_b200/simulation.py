@@ -261,6 +261,14 @@ class Simulation:
         self._check(self.lib.pic_solve_initial_field(self.ctx, rel_tol, max_iter, out, L.NPOISSON))
         return dict(iterations=int(out[0]), rel_residual=out[1], mean_rho=out[2], gauss_max=out[3])
 
+    def particle_order_stats(self, kind: int) -> dict:
+        """Visitor lists and stragglers of the tiled kernel
+        (pic_particle_order_stats)."""
+        out = (ctypes.c_int64 * 4)()
+        self._check(self.lib.pic_particle_order_stats(self.ctx, kind, out, 4))
+        return dict(visitors=int(out[0]), lists_complete=bool(out[1]), pushes_since_sort=int(out[2]),
+                    global_kernel=int(out[3]))
+
     # -- profiling ------------------------------------------------------------------
     def profile(self, on: bool = True):
         self._check(self.lib.pic_profile_enable(self.ctx, 1 if on else 0))
