@@ -327,6 +327,7 @@ def laser_bench(local, rank, warmup_steps, steps, precision, cells=(256, 128, 12
     npart0 = sum(sim.num_particles(k) for k in range(2))
     ms, kern, _ = run_case(sim, warmup_steps, steps)
     npart = sum(sim.num_particles(k) for k in range(2))
+    order = [sim.particle_order_stats(k) for k in range(2)]
     sim.close()
     peak, peak_kind = measured_peaks()
     ncell = w.nx * w.ny * w.nz
@@ -334,7 +335,7 @@ def laser_bench(local, rank, warmup_steps, steps, precision, cells=(256, 128, 12
     return {"workload": w.name, "precision": precision, "timed_after_step": warmup_steps + 1,
             "particles_at_start": npart0, "particles_timed": npart,
             "particle_steps_per_s": npart * steps / (ms / 1e3), "ms_per_step": ms / steps,
-            "tile_push_roofline_frac": roof["frac"] if roof else None,
+            "tile_push_roofline_frac": roof["frac"] if roof else None, "particle_order": order,
             "kernels": {k: {"ms_total": v[0], "launches": v[1]} for k, v in kern.items()}}
 
 

@@ -71,8 +71,9 @@ typedef struct PicParams {
     int32_t laser_envelope;    /* extension: 0 sine envelope (boundary.cpp:13), 1 Gaussian with intensity FWHM laser_pulse_duration */
     int32_t laser_profile;     /* extension: 0 Gaussian beam (boundary.cpp:38), 1 cubic-B-spline amplitude grid */
     int32_t tile;              /* edge of the shared-memory particle tile in cells (0: default 4, <0: no tiling) */
-    int32_t sort_interval;     /* pushes between full counting sorts of the particles by tile (0: default 4);
-                                  between sorts each push re-bins only the particles that changed tile */
+    int32_t sort_interval;     /* pushes between full counting sorts of the particles by tile (0: default 4,
+                                  1 in adjoint contexts); between sorts each push re-bins only the particles
+                                  that changed tile */
     int32_t adjoint;           /* 1: adjoint-capable context (stable particle order, removal marks particles dead;
                                   absorbing faces only); see pic_adjoint_* */
     int32_t absorbing;         /* extension: 1 = Silver-Mueller absorbing condition on every non-periodic face

@@ -420,7 +420,10 @@ int pic_create(const PicParams *pp, int device, pic_ctx **out) {
     // shared-memory path, but the kernel slows as the order decays (the
     // thermal plasma: 10.8 ms per launch 4 pushes after a sort, 12.4 ms 64
     // pushes after); a sort every 4 pushes measured fastest overall.
-    c->sort_interval = p.sort_interval > 0 ? p.sort_interval : 4;
+    // Adjoint contexts have no visitor lists: they sort before every push,
+    // so that no particle leaves the shared-memory path of the forward or
+    // of the reverse sweep (each sort's permutation goes on the tape).
+    c->sort_interval = p.sort_interval > 0 ? p.sort_interval : (p.adjoint ? 1 : 4);
     if (c->tile > 0) {
         for (int d = 0; d < 3; ++d) c->ntile[d] = (n[d] + c->tile - 1) / c->tile;
         c->nkeys = (long long)c->ntile[0] * c->ntile[1] * c->ntile[2] * kOctants * c->tile * c->tile * c->tile;

@@ -263,10 +263,18 @@ __device__ __forceinline__ void atomic_add(float *p, float v) { atomicAdd(p, v);
 //   GlobalAcc: hardware atomics into the global ring buffers (coef 1).
 //   FixedAcc:  a CTA's shared-memory tile; values come scaled by
 //              coef(c) = scale[c], are rounded to a 64-bit integer and split
-//              into 20-bit limbs added with native 32-bit integer atomics
+//              into 18-bit limbs added with native 32-bit integer atomics
 //              (NL = 2 limbs for FP32, 3 for FP64).  Integer sums do not
 //              depend on the order of the additions.  (Shared-memory 64-bit
 //              integer atomics measured 2.6x slower on the whole kernel.)
+// One contribution stays below 2^kFixedBits (31 FP32, 49 FP64), so that
+// 16383 additions per point fit: the unsigned 18-bit limb sums in 32 bits,
+// the signed top limb sums (below 2^13 resp. 2^15 each) in 32 bits, and
+// the reassembled total in 64 bits.
+constexpr int kLimbBits = 18;
+constexpr unsigned kLimbMask = (1u << kLimbBits) - 1u;
+template <typename real>
+constexpr int fixed_bits() { return sizeof(real) == 8 ? 49 : 31; }
 template <typename real>
 struct GlobalAcc {
     real *p[4];  // jx, jy, jz, rho (rho may be null)
@@ -281,12 +289,12 @@ struct FixedAcc {
     unsigned *p[4];   // limb 0 of jx, jy, jz, rho; limb l at + l * lstride
     int lstride;
     int sy, sz, o;
-    real scale[4];    // per component: |value * scale| < 2^(20*NL - 9)
+    real scale[4];    // per component: |value * scale| < 2^fixed_bits
     __device__ __forceinline__ bool has_rho() const { return p[3] != nullptr; }
     __device__ __forceinline__ real coef(int c) const { return scale[c]; }
     // q is already scaled.  Rounded to the nearest integer and split into
-    // limbs q = l2*2^40 + l1*2^20 + l0 (FP64) or q = h*2^20 + l0 (FP32),
-    // with l0, l1 in [0, 2^20) and the top limb signed.  FP64 rounds by the
+    // limbs q = l2*2^36 + l1*2^18 + l0 (FP64) or q = h*2^18 + l0 (FP32),
+    // with l0, l1 in [0, 2^18) and the top limb signed.  FP64 rounds by the
     // add-a-magic-constant method (the sum's low mantissa bits are the
     // integer), FP32 by a float-to-int conversion.  Zeros are added like
     // any value: a per-point zero test measured 10-20 % slower than the
@@ -295,13 +303,13 @@ struct FixedAcc {
         unsigned *a = p[c] + idx;
         if constexpr (NL == 3) {                                           // |q| < 2^51
             const long long qi = __double_as_longlong(q + 6755399441055744.0) - 0x4338000000000000LL;
-            atomicAdd(a, (unsigned)(qi & 0xFFFFF));
-            atomicAdd(a + lstride, (unsigned)((qi >> 20) & 0xFFFFF));
-            atomicAdd(a + 2 * lstride, (unsigned)(int)(qi >> 40));
+            atomicAdd(a, (unsigned)qi & kLimbMask);
+            atomicAdd(a + lstride, (unsigned)(qi >> kLimbBits) & kLimbMask);
+            atomicAdd(a + 2 * lstride, (unsigned)(int)(qi >> (2 * kLimbBits)));
         } else {                                                           // |q| < 2^31
             const int qi = __float2int_rn(q);
-            atomicAdd(a, (unsigned)qi & 0xFFFFFu);
-            atomicAdd(a + lstride, (unsigned)(qi >> 20));
+            atomicAdd(a, (unsigned)qi & kLimbMask);
+            atomicAdd(a + lstride, (unsigned)(qi >> kLimbBits));
         }
     }
 };

@@ -432,10 +432,10 @@ static void prepare_push(pic_ctx *c, int mask) {
 // limbs of the shared-memory fixed-point accumulators
 template <typename real>
 constexpr int limbs() { return sizeof(real) == 8 ? 3 : 2; }
-// |value * scale| stays below 2^(20*NL - 9): with at most kMaxTileParticles
-// additions per point the 20-bit limb sums fit in 32 bits and the
-// reassembled total in 64 bits
-constexpr int kMaxTileParticles = 4095;
+// |value * scale| stays below 2^fixed_bits: with at most kMaxTileParticles
+// additions per point the limb sums fit in 32 bits and the reassembled
+// total in 64 bits (FixedAcc)
+constexpr int kMaxTileParticles = 16383;
 
 // Asynchronous global -> shared copies (cp.async): a CTA issues every copy
 // of a batch without waiting on any, then waits once.  src_bytes 0 fills the
@@ -652,11 +652,13 @@ __global__ void __launch_bounds__(tile_threads<real>(), (tile_min_blocks<real, P
         int lz = l / D2, r = l - lz * D2, ly = r / DE, lx = r - ly * DE;
         const unsigned *q = sa + c * NL * DS + lz * dsz + ly * dsy + lx;
         long long tot;
-        if constexpr (NL == 2) tot = ((long long)(int)q[DS] << 20) + (long long)q[0];
-        else tot = ((long long)(int)q[2 * DS] << 40) + ((long long)q[DS] << 20) + (long long)q[0];
+        if constexpr (NL == 2) tot = ((long long)(int)q[DS] << kLimbBits) + (long long)q[0];
+        else
+            tot = ((long long)(int)q[2 * DS] << (2 * kLimbBits)) + ((long long)q[DS] << kLimbBits) + (long long)q[0];
         if (tot == 0) continue;
         int x = dO[0] + lx, y = dO[1] + ly, z = dO[2] + lz;
-        const real v = (real)((double)tot * ta.inv_scale[c < 3 ? c : 3]);
+        // FP32: single-precision arithmetic (the sum rounded to 24 bits)
+        const real v = (real)tot * (real)ta.inv_scale[c < 3 ? c : 3];
         if (x >= -1 && x <= g.f[0] && y >= -1 && y <= g.f[1] && z >= -1 && z <= g.f[2])
             atomic_add(ta.ring[c] + g.ri(z, y, x), v);
         else
@@ -719,7 +721,7 @@ static void tile_push_t(pic_ctx *c, int mask) {
     // Esirkepov weight are both within [-1, 1]) or |q w| smax^3 (rho, smax the
     // largest shape weight: 3/4 at 2nd order, 115/192 at 4th)
     const double dmax = std::max(c->p.dx, std::max(c->p.dy, c->p.dz));
-    const double lim = std::ldexp(1.0, 20 * limbs<real>() - 9);
+    const double lim = std::ldexp(1.0, fixed_bits<real>());
     const double smax = P == 3 ? 0.75 : 115.0 / 192.0;
     const double bj = 1.01 * qw_max * dmax / c->p.dt, br = 1.01 * qw_max * smax * smax * smax;
     for (int k = 0; k < 4; ++k) {

@@ -14,8 +14,9 @@ L2 1e-10 (FP64) / 1e-5 (FP32).
   lambda/10 cells, a0 = 2, 8 + 8 particles per cell, 4th order, absorbing
   faces): the GPU runs 200 steps (the pulse fills the box and the
   electrons move relativistically), then steps 201-204 are teacher-forced.
-* A clustered input whose one tile holds more than 4095 particles: that
-  tile takes the global-memory path as a whole.
+* Clustered inputs whose one tile holds 5000 particles (shared-memory
+  path, dense) and more than 16383 particles (that tile takes the
+  global-memory path as a whole).
 """
 import numpy as np
 import pytest
@@ -152,9 +153,10 @@ def _clustered(n_in_tile=5000, seed=3):
     return w, parts
 
 
+@pytest.mark.parametrize("n_in_tile", [5000, 17000])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_tile_over_4095_particles_takes_the_global_path(precision):
-    w, parts = _clustered()
+def test_crowded_tiles(precision, n_in_tile):
+    w, parts = _clustered(n_in_tile)
     states, _ = O.run_oracle(w, parts, 3)
     pairs = {n: (states[n], states[n + 1]) for n in range(3)}
     _teacher_forced(w, pairs, precision)
