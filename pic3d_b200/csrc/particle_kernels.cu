@@ -31,10 +31,10 @@ __global__ void __launch_bounds__(256) push_kernel(PushArgs<real> a) {
             set_status(a.status, ST_OOB);
             continue;
         }
-        int cn[3];
         const PmSrc<real> pm{a.px, a.py, a.pz, a.w, p};
-        if (push_body<real, P, SPIN, true>(a, p, o, pm, fv, acc, cn) && a.idx_pairs)
-            vis_note(a.vsink, a.g, (int)p, a.idx[2 * t + 1], cn);
+        push_body<real, P, SPIN, true>(a, p, o, pm, fv, acc, [&](const int (&cn)[3]) {
+            if (a.idx_pairs) vis_note(a.vsink, a.g, (int)p, a.idx[2 * t + 1], cn);
+        });
     }
 }
 

@@ -534,12 +534,14 @@ __device__ __forceinline__ void decode_old(const PushArgs<real> &a, long long p,
 // store, spin.  fv: the six field views; jv: view for the current arrays
 // (jx..rho share its strides).
 // Returns false when the particle was skipped (non-finite momentum or a move
-// over a cell: status set, nothing stored); else cnew is its new cell as the
-// next push's decode will see it.
-template <typename real, int P, bool SPIN, bool LDG, class Acc>
+// over a cell: status set, nothing stored).  The new state is stored before
+// the deposit (fewer values live through its loops); note(cnew) is called
+// then with the new cell as the next push's decode will see it.
+template <typename real, int P, bool SPIN, bool LDG, class Acc, class Note>
 __device__ __forceinline__ bool push_body(const PushArgs<real> &a, long long p, const OldPos<real> &o,
                                           const PmSrc<real> &pm, const View<const real> (&fv)[6], const Acc &acc,
-                                          int (&cnew)[3]) {
+                                          Note &&note) {
+    int cnew[3];
     constexpr bool F64 = cuda::std::is_same<real, double>::value;
     constexpr int H = P / 2;
     const Geom &g = a.g;
@@ -617,23 +619,6 @@ __device__ __forceinline__ bool push_body(const PushArgs<real> &a, long long p, 
         set_status(a.status, fin ? ST_CFL : ST_NAN);
         return false;
     }
-    const real qw = a.charge * pm.w[pm.i];
-    Axis1D<real, P> ax[3];
-    bool moved = false;
-    if constexpr (F64) {
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            axis_from_offsets<real, P>(o.ip[d], o.dp[d], i2[d], d2[d], ax[d]);
-            moved = moved || i2[d] != o.ip[d] || d2[d] != o.dp[d];
-        }
-    } else {
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            axis_from_move<P>(o.ip[d], o.dp[d], disp[d], i2[d], ax[d]);
-            moved = moved || disp[d] != real(0);
-        }
-    }
-    deposit<real, P>(acc, a.d_dt, ax, moved, qw);
     // store
     a.px[p] = pxn;
     a.py[p] = pyn;
@@ -664,6 +649,24 @@ __device__ __forceinline__ bool push_body(const PushArgs<real> &a, long long p, 
         a.oy1[p] = on[1];
         a.oz1[p] = on[2];
     }
+    note(cnew);
+    const real qw = a.charge * pm.w[pm.i];
+    Axis1D<real, P> ax[3];
+    bool moved = false;
+    if constexpr (F64) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            axis_from_offsets<real, P>(o.ip[d], o.dp[d], i2[d], d2[d], ax[d]);
+            moved = moved || i2[d] != o.ip[d] || d2[d] != o.dp[d];
+        }
+    } else {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            axis_from_move<P>(o.ip[d], o.dp[d], disp[d], i2[d], ax[d]);
+            moved = moved || disp[d] != real(0);
+        }
+    }
+    deposit<real, P>(acc, a.d_dt, ax, moved, qw);
     // electron spin precession (particle.cpp:318-368)
     if constexpr (SPIN) {
         if (a.electron) {

@@ -474,20 +474,23 @@ struct TileArgs {
 };
 
 // Threads per CTA and CTAs per SM the register allocation must allow.
-// FP32: two CTAs of 256 threads (measured 1.46x faster at 4th order than
-// one CTA with more registers).  FP64: its 143 KB of shared memory allows
-// one CTA per SM; 512 threads at 128 registers (a few spills) measured 12 %
-// faster on the laser workload than 256 at 237 registers, while 384 lost
-// (a tile's 512 particles per species then leave a third of the second
-// round idle).
-// Three FP32 CTAs per SM at 2nd order measured slower than two.
-template <typename real, int P = 5>
-constexpr int tile_min_blocks() { return sizeof(real) == 4 ? 2 : 1; }
-template <typename real>
-constexpr int tile_threads() { return sizeof(real) == 4 ? 256 : 512; }
+// Two CTAs of 256 threads (128 registers) where the shared memory of two
+// fits: FP32 (measured 1.46x faster at 4th order than one CTA with more
+// registers) and FP64 at 2nd order (107 KB per CTA on a step without rho;
+// 15.6 vs 19.4 ms per launch on the 256x128x128 thermal plasma against one
+// CTA of 512), while one CTA of the other overlaps its staging and flush.
+// FP64 at 4th order (160 KB) allows one CTA per SM: 512 threads at 128
+// registers (a few spills) measured 12 % faster on the laser workload than
+// 256 at 237 registers, while 384 lost (a tile's 512 particles per species
+// then leave a third of the second round idle).  Three FP32 CTAs per SM at
+// 2nd order measured slower than two.
+template <typename real, int P>
+constexpr int tile_min_blocks() { return sizeof(real) == 4 || P == 3 ? 2 : 1; }
+template <typename real, int P>
+constexpr int tile_threads() { return sizeof(real) == 4 || P == 3 ? 256 : 512; }
 
 template <typename real, int P, bool SPIN>
-__global__ void __launch_bounds__(tile_threads<real>(), (tile_min_blocks<real, P>())) tile_push_kernel(TileArgs<real> ta) {
+__global__ void __launch_bounds__(tile_threads<real, P>(), (tile_min_blocks<real, P>())) tile_push_kernel(TileArgs<real> ta) {
     constexpr int H = P / 2;
     constexpr int NL = limbs<real>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -502,8 +505,8 @@ __global__ void __launch_bounds__(tile_threads<real>(), (tile_min_blocks<real, P
     // and the (index, home tile) of each lane's particle per slot
     using PWord = typename PartIn<real>::word;
     constexpr int KW = PartIn<real>::kWords;
-    PWord *sp_in = reinterpret_cast<PWord *>(sa + particle_buffer_offset(5 * NL * DS)) + (threadIdx.x >> 5) * 2 * KW * 32;
-    int2 *sp_loc = reinterpret_cast<int2 *>(reinterpret_cast<PWord *>(sa + particle_buffer_offset(5 * NL * DS)) +
+    PWord *sp_in = reinterpret_cast<PWord *>(sa + particle_buffer_offset(ta.t.nacc * NL * DS)) + (threadIdx.x >> 5) * 2 * KW * 32;
+    int2 *sp_loc = reinterpret_cast<int2 *>(reinterpret_cast<PWord *>(sa + particle_buffer_offset(ta.t.nacc * NL * DS)) +
                                             (blockDim.x >> 5) * 2 * KW * 32) + (threadIdx.x >> 5) * 2 * 32;
     const int nacc = ta.t.nacc;
     const int tile = blockIdx.x;
@@ -623,12 +626,12 @@ __global__ void __launch_bounds__(tile_threads<real>(), (tile_min_blocks<real, P
                 if (!in_buffers(g, o, H)) {
                     set_status(a.status, ST_OOB);
                 } else if (inside && use_smem) {
-                    int cn[3];
                     constexpr int mo = PartIn<real>::kPos;   // momenta, then weight
                     const real *pr = reinterpret_cast<const real *>(sp_in + slot * KW * 32);
                     const PmSrc<real> pm{pr + mo * 32, pr + (mo + 1) * 32, pr + (mo + 2) * 32, pr + (mo + 3) * 32, lane};
-                    if (push_body<real, P, SPIN, false>(a, p, o, pm, fs, af, cn))
+                    push_body<real, P, SPIN, false>(a, p, o, pm, fs, af, [&](const int (&cn)[3]) {
                         vis_note(ta.vsink[k], g, (int)p, home, cn, tile, t0);
+                    });
                 } else if (!inside && idx < mh && vvalid[k]) {
                     // away from home: pushed from the visitor list of the tile it is in
                 } else {
@@ -687,9 +690,12 @@ TileBoxes tile_boxes(const pic_ctx *c) {
 size_t tile_smem_bytes(const pic_ctx *c) {
     const TileGeom t = tile_layout(c);
     const size_t rs = c->fp32 ? 4 : 8, nl = c->fp32 ? 2 : 3;
-    const size_t warps = (c->fp32 ? tile_threads<float>() : tile_threads<double>()) / 32;
+    const bool o2 = c->order == 2;
+    const size_t warps = (c->fp32 ? (o2 ? tile_threads<float, 3>() : tile_threads<float, 5>())
+                                  : (o2 ? tile_threads<double, 3>() : tile_threads<double, 5>())) / 32;
     const size_t words = c->fp32 ? PartIn<float>::kWords : PartIn<double>::kWords;
-    return 6 * (size_t)t.gsize * rs + 4 * (size_t)particle_buffer_offset((int)(5 * nl * t.dsize)) +
+    // the accumulators of this launch: jx, jy, jz, and rho0, rho1 on a step whose rho is observed
+    return 6 * (size_t)t.gsize * rs + 4 * (size_t)particle_buffer_offset((int)(t.nacc * nl * t.dsize)) +
            warps * 2 * 32 * (words * rs + sizeof(int2));
 }
 
@@ -743,7 +749,7 @@ static void tile_push_t(pic_ctx *c, int mask) {
     size_t smem = tile_smem_bytes(c);
     cudaFuncSetAttribute(tile_push_kernel<real, P, SPIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int ntiles = c->ntile[0] * c->ntile[1] * c->ntile[2];
-    tile_push_kernel<real, P, SPIN><<<ntiles, tile_threads<real>(), smem, c->stream>>>(ta);
+    tile_push_kernel<real, P, SPIN><<<ntiles, tile_threads<real, P>(), smem, c->stream>>>(ta);
 }
 
 // the counts pic_particle_order_stats reports (host side, synchronising)
