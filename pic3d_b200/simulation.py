@@ -266,7 +266,7 @@ class Simulation:
         (pic_particle_order_stats)."""
         out = (ctypes.c_int64 * 4)()
         self._check(self.lib.pic_particle_order_stats(self.ctx, kind, out, 4))
-        return dict(visitors=int(out[0]), lists_complete=bool(out[1]), pushes_since_sort=int(out[2]),
+        return dict(visitors=int(out[0]), lists_used=bool(out[1]), pushes_since_sort=int(out[2]),
                     global_kernel=int(out[3]))
 
     # -- profiling ------------------------------------------------------------------

@@ -8,8 +8,9 @@ by the CTA of the tile it is in (the role the reference's particle exchange
 plays between ranks, src/mpi_utils.cpp:62-230, inside one GPU).  Removal at
 absorbing faces compacts the arrays; the compaction drops the entries of
 removed and moved particles and records the moved ones anew.  Lists that
-would overflow (more than half of the particles away from home) make the
-next push hand the particles away from home to the global-memory kernel.
+would overflow (more than half of the particles away from home) or name
+fewer than 3 % of the particles make the next push hand the particles away
+from home to the global-memory kernel.
 
 Free runs of a hot thermal plasma (most particles change tile) with the
 full sort every push, every 4 pushes (default) and never after the first,
@@ -95,9 +96,11 @@ def test_lists_stay_complete_within_their_capacity():
         stats.append(sim.particle_order_stats(0))
     got = sim.state()
     sim.close()
-    assert all(s["lists_complete"] for s in stats)
-    assert all(s["global_kernel"] == 0 for s in stats)
-    assert stats[-1]["visitors"] > 0.02 * len(parts[0]), stats[-1]
+    # a push that takes the particles away from home from the lists leaves
+    # none to the global kernel; past a few pushes the lists are in use
+    assert all(b["global_kernel"] == 0 for a, b in zip(stats, stats[1:]) if a["lists_used"])
+    assert all(s["lists_used"] for s in stats[6:])
+    assert stats[-1]["visitors"] > 0.03 * len(parts[0]), stats[-1]
     errs = array_errors(got, states[-1])
     assert max(errs.values()) < 1e-8, errs
 
@@ -116,7 +119,8 @@ def test_fp32_free_run_matches_sorted_every_push(hot_run, path):
 def test_removal_keeps_the_lists_complete():
     """Absorbing x faces: particles leave every step; the compaction moves
     particles into the holes and re-records them, the lists stay complete
-    and the run matches the oracle."""
+    (the pushes that use them leave nothing to the global kernel) and the run
+    matches the oracle."""
     w = _hot(2).with_(period=(0, 1, 1), u_th=(0.2, 0.0), name="hot_absorbing_x")
     parts = W.make_particles(w, seed=5)
     states, _ = O.run_oracle(w, parts, 20)
@@ -133,9 +137,9 @@ def test_removal_keeps_the_lists_complete():
     got = sim.state()
     sim.close()
     assert counts[-1] < counts[0] < len(parts[0])   # particles left through the faces during the run
-    assert all(s["lists_complete"] for s in stats)
-    assert all(s["global_kernel"] == 0 for s in stats)
-    assert max(s["visitors"] for s in stats) > 0
+    used = [a["lists_used"] for a in stats[:-1]]
+    assert sum(used) >= 8
+    assert all(b["global_kernel"] == 0 for a, b in zip(stats, stats[1:]) if a["lists_used"])
     errs = array_errors(got, ref)
     assert max(errs.values()) < 1e-8, errs
     perr, merr = particle_errors(got["particles"][0], ref["particles"][0], periods(w.params()))
