@@ -43,11 +43,19 @@ struct TileGeom {
 // (mod 2T*T) those 32 cells start in 32 different banks, so a warp's loads
 // and atomics at a common stencil offset are conflict-free (2 wavefronts
 // per 8-byte access, the minimum).
-static inline void padded_strides(int e, int T, int &sy, int &sz) {
-    sy = e;
+__host__ __device__ constexpr int padded_row(int e, int T) {
+    int sy = e;
     while (sy % (2 * T) != T) ++sy;
-    sz = e * sy;
+    return sy;
+}
+__host__ __device__ constexpr int padded_plane(int e, int T) {
+    int sz = e * padded_row(e, T);
     while (sz % (2 * T * T) != (T * T) % (2 * T * T)) ++sz;
+    return sz;
+}
+static inline void padded_strides(int e, int T, int &sy, int &sz) {
+    sy = padded_row(e, T);
+    sz = padded_plane(e, T);
 }
 
 template <int P>
@@ -501,16 +509,29 @@ constexpr int tile_min_blocks() { return sizeof(real) == 4 || P == 3 ? 2 : 1; }
 template <typename real, int P>
 constexpr int tile_threads() { return sizeof(real) == 4 || P == 3 ? 256 : 512; }
 
-template <typename real, int P, bool SPIN>
+// TT: the tile edge as a compile-time constant (0: from the arguments).
+// With the edge known, every stride of the shared boxes is a constant and
+// the stencil addresses fold into instruction offsets.
+template <typename real, int P, bool SPIN, int TT>
 __global__ void __launch_bounds__(tile_threads<real, P>(), (tile_min_blocks<real, P>())) tile_push_kernel(TileArgs<real> ta) {
     constexpr int H = P / 2;
     constexpr int NL = limbs<real>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     real *sf = reinterpret_cast<real *>(smem_raw);
     const Geom &g = ta.sp[0].g;
-    const int T = ta.t.T;
+    const int T = TT > 0 ? TT : ta.t.T;
     const int GE = gather_extent<P>(T), DE = deposit_extent<P>(T);
-    const int gsy = ta.t.gsy, gsz = ta.t.gsz, GS = ta.t.gsize, dsy = ta.t.dsy, dsz = ta.t.dsz, DS = ta.t.dsize;
+    int gsy, gsz, GS, dsy, dsz, DS;
+    if constexpr (TT > 0) {
+        constexpr int ge = gather_extent<P>(TT), de = deposit_extent<P>(TT);
+        constexpr int gy = padded_row(ge, TT), gz = padded_plane(ge, TT);
+        constexpr int dy = padded_row(de, TT), dz = padded_plane(de, TT);
+        gsy = gy; gsz = gz; GS = ge * gz;
+        dsy = dy; dsz = dz; DS = de * dz;
+    } else {
+        gsy = ta.t.gsy; gsz = ta.t.gsz; GS = ta.t.gsize;
+        dsy = ta.t.dsy; dsz = ta.t.dsz; DS = ta.t.dsize;
+    }
     const int G2 = GE * GE, G3 = G2 * GE, D2 = DE * DE, D3 = D2 * DE;
     unsigned *sa = reinterpret_cast<unsigned *>(sf + 6 * GS);   // [component][limb][DS]
     // per warp, two slots of one batch of particle inputs, [word][lane],
@@ -759,9 +780,14 @@ static void tile_push_t(pic_ctx *c, int mask) {
     ta.nstrag = c->d_nstrag;
     cudaMemsetAsync(c->d_nstrag, 0, 2 * sizeof(unsigned long long), c->stream);
     size_t smem = tile_smem_bytes(c);
-    cudaFuncSetAttribute(tile_push_kernel<real, P, SPIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int ntiles = c->ntile[0] * c->ntile[1] * c->ntile[2];
-    tile_push_kernel<real, P, SPIN><<<ntiles, tile_threads<real, P>(), smem, c->stream>>>(ta);
+    if (c->tile == 4) {   // the default edge: strides as constants
+        cudaFuncSetAttribute(tile_push_kernel<real, P, SPIN, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        tile_push_kernel<real, P, SPIN, 4><<<ntiles, tile_threads<real, P>(), smem, c->stream>>>(ta);
+    } else {
+        cudaFuncSetAttribute(tile_push_kernel<real, P, SPIN, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        tile_push_kernel<real, P, SPIN, 0><<<ntiles, tile_threads<real, P>(), smem, c->stream>>>(ta);
+    }
 }
 
 // the counts pic_particle_order_stats reports (host side, synchronising)
