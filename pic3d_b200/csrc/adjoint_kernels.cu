@@ -621,9 +621,20 @@ __device__ __forceinline__ void fixed_add(unsigned *a, int lstride, real q) {
     }
 }
 
-template <typename real, int P>
-__global__ void __launch_bounds__(256, 1) adj_tile_kernel(AdjPushArgs<real> a, AdjTileGeom t, const unsigned *toffs,
+// TT: the tile edge as a compile-time constant (0: from tg), which makes
+// every shared-box stride a constant.
+template <typename real, int P, int TT>
+__global__ void __launch_bounds__(256, 1) adj_tile_kernel(AdjPushArgs<real> a, AdjTileGeom tg, const unsigned *toffs,
                                                           int *strag, unsigned long long *nstrag) {
+    AdjTileGeom t = tg;
+    if constexpr (TT > 0) {
+        constexpr int ge = TT + 2 * (P / 2) + 1, de = TT + 2 * (P / 2) + 3;
+        constexpr int gy = padded_row(ge, TT), gz = padded_plane(ge, TT);
+        constexpr int dy = padded_row(de, TT), dz = padded_plane(de, TT);
+        t.T = TT; t.GE = ge; t.DE = de;
+        t.gsy = gy; t.gsz = gz; t.gsize = ge * gz;
+        t.dsy = dy; t.dsz = dz; t.dsize = de * dz;
+    }
     constexpr int H = P / 2, NL = adj_limbs<real>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Geom &g = a.g;
@@ -1315,9 +1326,14 @@ static void adj_push_launch(pic_ctx *c, AdjState *A, const Blob &b, int kind, in
         cudaMemsetAsync(c->d_nstrag + kind, 0, sizeof(unsigned long long), c->stream);
         prof_begin(c, "adjoint_tile_push_deposit");
         if (tg.cap > 0) {
-            cudaFuncSetAttribute(adj_tile_kernel<real, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            adj_tile_kernel<real, P><<<ntiles, 256, smem, c->stream>>>(
-                a, tg, (const unsigned *)blob_part(b, b.toff_part[kind]), s.strag, c->d_nstrag + kind);
+            const unsigned *toffs = (const unsigned *)blob_part(b, b.toff_part[kind]);
+            if (c->tile == 4) {   // the default edge: strides as constants
+                cudaFuncSetAttribute(adj_tile_kernel<real, P, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                adj_tile_kernel<real, P, 4><<<ntiles, 256, smem, c->stream>>>(a, tg, toffs, s.strag, c->d_nstrag + kind);
+            } else {
+                cudaFuncSetAttribute(adj_tile_kernel<real, P, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                adj_tile_kernel<real, P, 0><<<ntiles, 256, smem, c->stream>>>(a, tg, toffs, s.strag, c->d_nstrag + kind);
+            }
             a.idx = s.strag;
             a.nidx = c->d_nstrag + kind;
         }

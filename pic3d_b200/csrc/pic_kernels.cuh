@@ -57,6 +57,20 @@ void launch_sort_due(pic_ctx *c, int mask);   // the sorts the next push of the 
 void launch_tile_push(pic_ctx *c, int mask);
 int tile_order_stats(pic_ctx *c, int kind, long long (&out)[4]);
 VisSink vis_sink_of(const pic_ctx *c, const Species &s);   // where a push of species s records visitors
+// Row and plane strides of a tile kernel's shared box of extent e for tile
+// edge T (padded so that 32 consecutive cells of a tile start in different
+// banks).
+__host__ __device__ constexpr int padded_row(int e, int T) {
+    int sy = e;
+    while (sy % (2 * T) != T) ++sy;
+    return sy;
+}
+__host__ __device__ constexpr int padded_plane(int e, int T) {
+    int sz = e * padded_row(e, T);
+    while (sz % (2 * T * T) != (T * T) % (2 * T * T)) ++sz;
+    return sz;
+}
+
 // the tile kernels' shared boxes: gather box of GE points per axis (row and
 // plane strides gsy, gsz, gsize elements), deposit box of DE (dsy, dsz, dsize)
 struct TileBoxes {

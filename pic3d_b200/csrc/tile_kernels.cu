@@ -43,16 +43,6 @@ struct TileGeom {
 // (mod 2T*T) those 32 cells start in 32 different banks, so a warp's loads
 // and atomics at a common stencil offset are conflict-free (2 wavefronts
 // per 8-byte access, the minimum).
-__host__ __device__ constexpr int padded_row(int e, int T) {
-    int sy = e;
-    while (sy % (2 * T) != T) ++sy;
-    return sy;
-}
-__host__ __device__ constexpr int padded_plane(int e, int T) {
-    int sz = e * padded_row(e, T);
-    while (sz % (2 * T * T) != (T * T) % (2 * T * T)) ++sz;
-    return sz;
-}
 static inline void padded_strides(int e, int T, int &sy, int &sz) {
     sy = padded_row(e, T);
     sz = padded_plane(e, T);
