@@ -2,9 +2,12 @@
 // memory, host <-> device conversion and the per-step orchestration of the
 // reference's run_main_time_loop (src/simulation.cpp:159-183).
 #include <algorithm>
+#include <atomic>
+#include <condition_variable>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -202,23 +205,127 @@ int ensure_pinned(pic_ctx *c, int64_t n) {
     return PIC_OK;
 }
 
-// memcpy of a large block split over a few host threads (host copies into
-// and out of the pinned buffers run at several times one core's rate)
-void par_memcpy(void *dst, const void *src, size_t bytes) {
-    const unsigned hw = std::thread::hardware_concurrency();
-    const int nt = bytes >= (4u << 20) ? (int)std::min(8u, hw > 0 ? hw : 1u) : 1;
-    if (nt <= 1) {
-        std::memcpy(dst, src, bytes);
-        return;
+// memcpy of a large block split over the host's cores.  Host copies into
+// and out of the pinned staging buffers run at several times one core's
+// rate; the worker threads live for the whole process (a copy of one 38 MB
+// chunk is too short to start threads for it).
+namespace {
+class CopyPool {
+  public:
+    static CopyPool &get() {
+        static CopyPool pool;
+        return pool;
     }
-    const size_t part = ((bytes + nt - 1) / nt + 63) & ~(size_t)63;
-    std::thread th[8];
-    for (int t = 1; t < nt; ++t) {
-        const size_t lo = std::min(bytes, part * t), hi = std::min(bytes, part * (t + 1));
-        th[t] = std::thread([=] { std::memcpy((char *)dst + lo, (const char *)src + lo, hi - lo); });
+    void copy(void *dst, const void *src, size_t bytes) {
+        const int np = bytes >= (4u << 20) ? nparts_ : 1;
+        if (np <= 1 || workers_.empty()) {
+            std::memcpy(dst, src, bytes);
+            return;
+        }
+        std::lock_guard<std::mutex> one_job(job_);   // callers on several host threads take turns
+        std::unique_lock<std::mutex> lk(m_);
+        dst_ = (char *)dst;
+        src_ = (const char *)src;
+        bytes_ = bytes;
+        part_ = ((bytes + np - 1) / np + 63) & ~(size_t)63;
+        nparts_job_ = np;
+        next_.store(0);
+        left_ = np;
+        ++gen_;
+        lk.unlock();
+        cv_.notify_all();
+        work();
+        lk.lock();
+        done_.wait(lk, [&] { return left_ == 0; });
     }
-    std::memcpy(dst, src, std::min(bytes, part));
-    for (int t = 1; t < nt; ++t) th[t].join();
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto &t : workers_) t.join();
+    }
+
+  private:
+    CopyPool() {
+        const unsigned hw = std::thread::hardware_concurrency();
+        nparts_ = (int)std::min(16u, hw > 0 ? hw : 1u);
+        for (int t = 1; t < nparts_; ++t) workers_.emplace_back([this] { loop(); });
+    }
+    // take parts of the current job until none is left
+    void work() {
+        int k;
+        while ((k = next_.fetch_add(1)) < nparts_job_) {
+            const size_t lo = std::min(bytes_, part_ * k), hi = std::min(bytes_, part_ * (k + 1));
+            if (hi > lo) std::memcpy(dst_ + lo, src_ + lo, hi - lo);
+            std::lock_guard<std::mutex> lk(m_);
+            if (--left_ == 0) done_.notify_one();
+        }
+    }
+    void loop() {
+        unsigned long long seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+            }
+            work();
+        }
+    }
+    std::vector<std::thread> workers_;
+    std::mutex job_, m_;
+    std::condition_variable cv_, done_;
+    char *dst_ = nullptr;
+    const char *src_ = nullptr;
+    size_t bytes_ = 0, part_ = 0;
+    int nparts_ = 1, nparts_job_ = 0, left_ = 0;
+    std::atomic<int> next_{0};
+    unsigned long long gen_ = 0;
+    bool stop_ = false;
+};
+}  // namespace
+
+void par_memcpy(void *dst, const void *src, size_t bytes) { CopyPool::get().copy(dst, src, bytes); }
+
+// A host <-> device copy of `bytes` through the two pinned staging buffers:
+// the host copy of one chunk overlaps the DMA of the other (a copy from or
+// to pageable memory runs at a few GB/s).
+static int staged_h2d(pic_ctx *c, void *dev, const void *host, size_t bytes) {
+    int r = ensure_pinned(c, kPinRecords);
+    if (r) return r;
+    const size_t chunk = (size_t)kPinRecords * 144;
+    for (size_t off = 0, i = 0; off < bytes; off += chunk, ++i) {
+        const size_t m = std::min(chunk, bytes - off);
+        const int b = (int)(i & 1);
+        CK(cudaEventSynchronize(c->pin_ev[b]));
+        par_memcpy(c->h_pin[b], (const char *)host + off, m);
+        CK(cudaMemcpyAsync((char *)dev + off, c->h_pin[b], m, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaEventRecord(c->pin_ev[b], c->stream));
+    }
+    return PIC_OK;
+}
+
+static int staged_d2h(pic_ctx *c, void *host, const void *dev, size_t bytes) {
+    int r = ensure_pinned(c, kPinRecords);
+    if (r) return r;
+    const size_t chunk = (size_t)kPinRecords * 144;
+    const size_t nch = (bytes + chunk - 1) / chunk;
+    auto enqueue = [&](size_t i) -> cudaError_t {
+        const size_t off = i * chunk, m = std::min(chunk, bytes - off);
+        cudaError_t e = cudaMemcpyAsync(c->h_pin[i & 1], (const char *)dev + off, m, cudaMemcpyDeviceToHost, c->stream);
+        return e != cudaSuccess ? e : cudaEventRecord(c->pin_ev[i & 1], c->stream);
+    };
+    if (nch) CK(enqueue(0));
+    for (size_t i = 0; i < nch; ++i) {
+        if (i + 1 < nch) CK(enqueue(i + 1));
+        CK(cudaEventSynchronize(c->pin_ev[i & 1]));
+        const size_t off = i * chunk;
+        par_memcpy((char *)host + off, c->h_pin[i & 1], std::min(chunk, bytes - off));
+    }
+    return PIC_OK;
 }
 
 int array_info(const pic_ctx *c, int which, void **dptr, long long *n) {
@@ -523,11 +630,12 @@ int pic_upload_array(pic_ctx *c, int which, const double *host) {
     long long n;
     if (array_info(c, which, &d, &n) != PIC_OK) return fail(c, PIC_EINVAL, "bad array id");
     if (!c->fp32) {
-        CK(cudaMemcpyAsync(d, host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        int r = staged_h2d(c, d, host, (size_t)n * sizeof(double));
+        if (r) return r;
     } else {
         int r = ensure_stage(c, (size_t)n * sizeof(double));
+        r = r ? r : staged_h2d(c, c->d_stage, host, (size_t)n * sizeof(double));
         if (r) return r;
-        CK(cudaMemcpyAsync(c->d_stage, host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         launch_convert_array(c, d, c->d_stage, n, 1);
     }
     CK(cudaStreamSynchronize(c->stream));
@@ -542,12 +650,14 @@ int pic_download_array(pic_ctx *c, int which, double *host) {
     if (array_info(c, which, &d, &n) != PIC_OK) return fail(c, PIC_EINVAL, "bad array id");
     int st = sync_status(c);
     if (!c->fp32) {
-        CK(cudaMemcpyAsync(host, d, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        int r = staged_d2h(c, host, d, (size_t)n * sizeof(double));
+        if (r) return r;
     } else {
         int r = ensure_stage(c, (size_t)n * sizeof(double));
         if (r) return r;
         launch_convert_array(c, c->d_stage, d, n, 0);
-        CK(cudaMemcpyAsync(host, c->d_stage, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        r = staged_d2h(c, host, c->d_stage, (size_t)n * sizeof(double));
+        if (r) return r;
     }
     CK(cudaStreamSynchronize(c->stream));
     return st;
