@@ -719,11 +719,15 @@ __global__ void __launch_bounds__(256, 1) adj_tile_kernel(AdjPushArgs<real> a, A
         if (!adj_particle<real, P, false>(a, p, fv, lj, lin)) continue;
         if (!a.scatter_fields) continue;
         flag[i] = 1;
+        // per component the largest magnitude of the tile: reduced over the
+        // warp's active lanes first, one shared atomic per warp
+        const unsigned am = __activemask();
+        const bool leader = (threadIdx.x & 31) == __ffs(am) - 1;
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
-            slin[i * 6 + c] = lin[3 + c];
-            const float mag = (float)fabs(lin[3 + c]);
-            atomicMax(smax + c, __float_as_uint(mag));
+            slin[c * t.cap + i] = lin[3 + c];
+            const unsigned mag = __reduce_max_sync(am, __float_as_uint((float)fabs(lin[3 + c])));
+            if (leader) atomicMax(smax + c, mag);
         }
     }
     if (!a.scatter_fields) return;
@@ -746,7 +750,7 @@ __global__ void __launch_bounds__(256, 1) adj_tile_kernel(AdjPushArgs<real> a, A
                              {ip[0], id[1], id[2]}, {id[0], ip[1], id[2]}, {id[0], id[1], ip[2]}};
 #pragma unroll 1
         for (int c = 0; c < 6; ++c) {
-            const real q = slin[i * 6 + c] * scale[c];
+            const real q = slin[c * t.cap + i] * scale[c];
             if (q == real(0)) continue;
             // dual axes: Ex x; Ey y; Ez z; Bx y, z; By x, z; Bz x, y
             const bool dx_ = c == 0 || c == 4 || c == 5, dy_ = c == 1 || c == 3 || c == 5,
