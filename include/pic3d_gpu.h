@@ -314,8 +314,8 @@ int pic_profile_reset(pic_ctx *ctx);
  *         their tile's slice of the sorted arrays, pushed from the list of
  *         the tile they are in);
  * out[1]: 1 if the next push takes the particles away from home from those
- *         lists (they are complete and name at least 3 % of the species;
- *         else the global kernel pushes them after the tiles);
+ *         lists (they are complete and, in FP64, name at least 3 % of the
+ *         species; else the global kernel pushes them after the tiles);
  * out[2]: pushes since the last full counting sort;
  * out[3]: particles the last push handed to the global-memory kernel.
  * Synchronises the context's stream.                                     */

@@ -285,23 +285,25 @@ __global__ void vis_scatter_kernel(const int *raw, const VisState *vs, long long
     }
 }
 
-// the lists just built are the ones the coming push reads; it records into
-// an empty raw list
-// Below this fraction of a species away from home, the particles away from
-// home are pushed by the global-memory kernel instead: on the 256x128x128
-// thermal plasma (1.4 % away 2 pushes after a sort) the visitor lists lost
-// 4 % (FP64 2nd order) to 6 % (FP64 4th order) of a step, because a tile's
-// few visitors add a partial round of batches; on the laser run (6 % away,
-// relativistic electrons) they won 6 % (FP32).
-constexpr double kVisitorMinFraction = 0.03;
+// FP64: below this fraction of a species away from home, the particles away
+// from home are pushed by the global-memory kernel instead.  On the
+// 256x128x128 thermal plasma (1.4 % away two pushes after a sort) the
+// visitor lists measured even at 2nd order and 4 % slower at 4th (a tile's
+// few visitors add a partial round of batches, and the FP64 kernel has the
+// longer rounds); on the laser run (6 % away, relativistic electrons) they
+// win.  FP32 uses them at any fraction (1.6 % faster at 2nd order, 2.6 % at
+// 4th on the thermal plasma).
+inline double visitor_min_fraction(const pic_ctx *c) { return c->fp32 ? 0.0 : 0.03; }
 
-__host__ __device__ inline bool visitor_lists_pay(unsigned long long entries, long long particles) {
-    return (double)entries >= kVisitorMinFraction * (double)particles;
+__host__ __device__ inline bool visitor_lists_pay(unsigned long long entries, long long particles, double min_frac) {
+    return (double)entries >= min_frac * (double)particles;
 }
 
-__global__ void vis_rotate_kernel(VisState *vs, long long cap, const long long *count) {
+// the lists just built are the ones the coming push reads; it records into
+// an empty raw list
+__global__ void vis_rotate_kernel(VisState *vs, long long cap, const long long *count, double min_frac) {
     vs->nvis = min((long long)vs->nraw, cap);
-    vs->valid_cur = vs->valid_next && visitor_lists_pay(vs->nvis, *count);
+    vs->valid_cur = vs->valid_next && visitor_lists_pay(vs->nvis, *count, min_frac);
     vs->nraw = 0;
     vs->valid_next = 1u;
 }
@@ -318,7 +320,7 @@ static void launch_vis_build(pic_ctx *c, Species &s) {
     scan_add_kernel<<<(unsigned)((nt + 1 + 255) / 256), 256, 0, c->stream>>>(s.vis_cnt, nt, c->d_blocksums, per_block,
                                                                              s.vis_off, s.vis_cnt);
     vis_scatter_kernel<<<grid, 256, 0, c->stream>>>(s.vraw, s.vs, s.vcap, s.vis_cnt, s.vis);
-    vis_rotate_kernel<<<1, 1, 0, c->stream>>>(s.vs, s.vcap, s.d_count);
+    vis_rotate_kernel<<<1, 1, 0, c->stream>>>(s.vs, s.vcap, s.d_count, visitor_min_fraction(c));
 }
 
 static TileGeom tile_geom(const pic_ctx *c) {
@@ -795,7 +797,8 @@ int tile_order_stats(pic_ctx *c, int kind, long long (&out)[4]) {
         if (cudaMemcpy(&n, s.d_count, sizeof n, cudaMemcpyDeviceToHost) != cudaSuccess) return PIC_ECUDA;
         const bool built = s.vis_built_for == s.pushes_since_sort;
         out[0] = built ? (long long)v.nvis : std::min<long long>((long long)v.nraw, s.vcap);
-        out[1] = built ? v.valid_cur : (v.valid_next && visitor_lists_pay((unsigned long long)out[0], n));
+        out[1] = built ? v.valid_cur
+                       : (v.valid_next && visitor_lists_pay((unsigned long long)out[0], n, visitor_min_fraction(c)));
     }
     if (c->d_nstrag) {
         unsigned long long ns[2] = {0, 0};
