@@ -485,7 +485,8 @@ struct TileArgs {
     VisSink vsink[2];
 };
 
-// Threads per CTA and CTAs per SM the register allocation must allow.
+// Threads per CTA of an ordinary step (the kernel's launch bounds ask for
+// two CTAs per SM at 256 threads, one at 512: 128 registers either way).
 // Two CTAs of 256 threads (128 registers) where the shared memory of two
 // fits: FP32 (measured 1.46x faster at 4th order than one CTA with more
 // registers) and FP64 at 2nd order (107 KB per CTA on a step without rho;
@@ -497,15 +498,14 @@ struct TileArgs {
 // then leave a third of the second round idle).  Three FP32 CTAs per SM at
 // 2nd order measured slower than two.
 template <typename real, int P>
-constexpr int tile_min_blocks() { return sizeof(real) == 4 || P == 3 ? 2 : 1; }
-template <typename real, int P>
 constexpr int tile_threads() { return sizeof(real) == 4 || P == 3 ? 256 : 512; }
 
 // TT: the tile edge as a compile-time constant (0: from the arguments).
 // With the edge known, every stride of the shared boxes is a constant and
 // the stencil addresses fold into instruction offsets.
-template <typename real, int P, bool SPIN, int TT>
-__global__ void __launch_bounds__(tile_threads<real, P>(), (tile_min_blocks<real, P>())) tile_push_kernel(TileArgs<real> ta) {
+// NT: threads per CTA of this instantiation (512: one CTA per SM)
+template <typename real, int P, bool SPIN, int TT, int NT>
+__global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) tile_push_kernel(TileArgs<real> ta) {
     constexpr int H = P / 2;
     constexpr int NL = limbs<real>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -712,12 +712,20 @@ TileBoxes tile_boxes(const pic_ctx *c) {
     return TileBoxes{t.GE, t.DE, t.gsy, t.gsz, t.gsize, t.dsy, t.dsz, t.dsize};
 }
 
+// Threads per CTA of a launch.  FP64 at 2nd order on a step whose rho is
+// observed: its five accumulators (131 KB per CTA) leave room for one CTA
+// per SM, so that CTA takes 512 threads instead of 256.
+static int tile_launch_threads(const pic_ctx *c) {
+    const bool o2 = c->order == 2;
+    if (!c->fp32 && o2 && tile_layout(c).nacc == 5) return 512;
+    return c->fp32 ? (o2 ? tile_threads<float, 3>() : tile_threads<float, 5>())
+                   : (o2 ? tile_threads<double, 3>() : tile_threads<double, 5>());
+}
+
 size_t tile_smem_bytes(const pic_ctx *c) {
     const TileGeom t = tile_layout(c);
     const size_t rs = c->fp32 ? 4 : 8, nl = c->fp32 ? 2 : 3;
-    const bool o2 = c->order == 2;
-    const size_t warps = (c->fp32 ? (o2 ? tile_threads<float, 3>() : tile_threads<float, 5>())
-                                  : (o2 ? tile_threads<double, 3>() : tile_threads<double, 5>())) / 32;
+    const size_t warps = (size_t)tile_launch_threads(c) / 32;
     const size_t words = c->fp32 ? PartIn<float>::kWords : PartIn<double>::kWords;
     // the accumulators of this launch: jx, jy, jz, and rho0, rho1 on a step whose rho is observed
     return 6 * (size_t)t.gsize * rs + 4 * (size_t)particle_buffer_offset((int)(t.nacc * nl * t.dsize)) +
@@ -773,13 +781,21 @@ static void tile_push_t(pic_ctx *c, int mask) {
     cudaMemsetAsync(c->d_nstrag, 0, 2 * sizeof(unsigned long long), c->stream);
     size_t smem = tile_smem_bytes(c);
     const int ntiles = c->ntile[0] * c->ntile[1] * c->ntile[2];
-    if (c->tile == 4) {   // the default edge: strides as constants
-        cudaFuncSetAttribute(tile_push_kernel<real, P, SPIN, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        tile_push_kernel<real, P, SPIN, 4><<<ntiles, tile_threads<real, P>(), smem, c->stream>>>(ta);
-    } else {
-        cudaFuncSetAttribute(tile_push_kernel<real, P, SPIN, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        tile_push_kernel<real, P, SPIN, 0><<<ntiles, tile_threads<real, P>(), smem, c->stream>>>(ta);
+    constexpr int NT = tile_threads<real, P>();
+    auto launch = [&](auto kernel, int threads) {
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kernel<<<ntiles, threads, smem, c->stream>>>(ta);
+    };
+    const bool wide = tile_launch_threads(c) != NT;
+    if constexpr (sizeof(real) == 8 && NT != 512) {
+        if (wide) {
+            if (c->tile == 4) launch(tile_push_kernel<real, P, SPIN, 4, 512>, 512);
+            else launch(tile_push_kernel<real, P, SPIN, 0, 512>, 512);
+            return;
+        }
     }
+    if (c->tile == 4) launch(tile_push_kernel<real, P, SPIN, 4, NT>, NT);   // the default edge: strides as constants
+    else launch(tile_push_kernel<real, P, SPIN, 0, NT>, NT);
 }
 
 // the counts pic_particle_order_stats reports (host side, synchronising)
